@@ -1,0 +1,286 @@
+// C ABI of libfastwigner: plan objects, step sequencing, error reporting.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+#include "fw_internal.h"
+#include "passes.cuh"
+
+namespace fw {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+int fail(int code, const std::string& msg) { set_error(msg); return code; }
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(FW_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// exp(-2 pi i k / N), k < N, computed in FP64 with the angle reduced exactly
+// through integer arithmetic on k (so the table is accurate to FP64 rounding).
+static std::vector<double> twiddles(int n) {
+  std::vector<double> t(2 * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    t[2 * k] = cos(a);
+    t[2 * k + 1] = sin(a);
+  }
+  return t;
+}
+
+static int upload_twiddles(int n, int dtype, void** dev) {
+  std::vector<double> t = twiddles(n);
+  cudaError_t e;
+  if (dtype == FW_F64) {
+    e = cudaMalloc(dev, t.size() * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(twiddles)");
+    e = cudaMemcpy(*dev, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice);
+  } else {
+    std::vector<float> f(t.begin(), t.end());
+    e = cudaMalloc(dev, f.size() * sizeof(float));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(twiddles)");
+    e = cudaMemcpy(*dev, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(twiddles)");
+  return FW_OK;
+}
+
+}  // namespace fw
+
+using namespace fw;
+
+struct fw_wigner_plan {
+  int P, X, batch, dtype;
+  int nparts;          // column-pass CTAs per instance (partials per instance)
+  void* twP = nullptr; // twiddles for length P
+  void* twX = nullptr; // twiddles for length X
+  double* ring = nullptr;  // 2 x batch x nparts x MMAX partial sums
+  double* wsum = nullptr;  // scratch for fw_wigner_weighted_sum partials
+  int wsum_blocks = 0;
+};
+
+static constexpr int MMAX = 2 + 8;
+
+extern "C" int fw_abi_version(void) { return FW_ABI_VERSION; }
+extern "C" const char* fw_last_error(void) { return g_err.c_str(); }
+extern "C" int fw_wigner_num_obs(int Mx, int Mp) { return 2 + Mx + Mp; }
+
+extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wigner_plan** out) {
+  if (out == nullptr) return fail(FW_EINVAL, "fw_wigner_plan_create: out is NULL");
+  *out = nullptr;
+  if (dtype != FW_F32 && dtype != FW_F64) return fail(FW_EINVAL, "fw_wigner_plan_create: dtype must be FW_F32 or FW_F64");
+  if (!size_supported(P) || !size_supported(X))
+    return fail(FW_EINVAL, "fw_wigner_plan_create: P_gridDIM and X_gridDIM must be powers of two in [128, 4096] (got " +
+                               std::to_string(P) + " x " + std::to_string(X) + ")");
+  if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_plan_create: batch must be in [1, 65535]");
+  const int np = col_parts(dtype, P, X);
+  if (np <= 0) return fail(FW_EINVAL, "fw_wigner_plan_create: unsupported X for the column pass tile");
+  fw_wigner_plan* p = new fw_wigner_plan();
+  p->P = P; p->X = X; p->batch = batch; p->dtype = dtype; p->nparts = np;
+  int rc = upload_twiddles(P, dtype, &p->twP);
+  if (rc == FW_OK) rc = upload_twiddles(X, dtype, &p->twX);
+  if (rc == FW_OK) {
+    cudaError_t e = cudaMalloc(&p->ring, sizeof(double) * 2 * (size_t)batch * np * MMAX);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(partials)");
+  }
+  if (rc == FW_OK) {
+    p->wsum_blocks = 256;
+    cudaError_t e = cudaMalloc(&p->wsum, sizeof(double) * 2 * (size_t)batch * p->wsum_blocks);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(weighted-sum scratch)");
+  }
+  if (rc != FW_OK) {
+    fw_wigner_plan_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return FW_OK;
+}
+
+extern "C" int fw_wigner_plan_destroy(fw_wigner_plan* p) {
+  if (p == nullptr) return FW_OK;
+  cudaFree(p->twP);
+  cudaFree(p->twX);
+  cudaFree(p->ring);
+  cudaFree(p->wsum);
+  delete p;
+  return FW_OK;
+}
+
+static inline const void* advance(const void* base, long long elems, size_t esz) {
+  return base == nullptr ? nullptr : static_cast<const char*>(base) + (ptrdiff_t)(elems * (long long)esz);
+}
+
+extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d, int steps, void* stream) {
+  if (plan == nullptr || d == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate: NULL plan or desc");
+  if (steps < 0) return fail(FW_EINVAL, "fw_wigner_propagate: steps must be >= 0");
+  if (steps == 0) return FW_OK;
+  if (d->W == nullptr || d->tabV == nullptr || d->tabK == nullptr)
+    return fail(FW_EINVAL, "fw_wigner_propagate: W, tabV and tabK are required");
+  if (d->Mx < 0 || d->Mx > 4 || d->Mp < 0 || d->Mp > 4) return fail(FW_EINVAL, "fw_wigner_propagate: Mx, Mp must be in [0, 4]");
+  if ((d->Mx > 0 && d->wx == nullptr) || (d->Mp > 0 && d->wp == nullptr))
+    return fail(FW_EINVAL, "fw_wigner_propagate: observable weights missing");
+  if (d->step_kind == FW_STEP_SPLIT && d->s0 == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate: split steps need s0");
+  if (d->step_kind != FW_STEP_FUSED && d->step_kind != FW_STEP_SPLIT) return fail(FW_EINVAL, "fw_wigner_propagate: bad step_kind");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t rs = plan->dtype == FW_F64 ? sizeof(double) : sizeof(float);
+  const size_t tes = d->tab_real ? rs : 2 * rs;
+  const int M = 2 + d->Mx + d->Mp;
+  const int B = plan->batch;
+  const size_t ring_slot = (size_t)B * plan->nparts * M;
+
+  PassArgs base{};
+  base.W = d->W;
+  base.w_bs = d->w_bstride;
+  base.P = plan->P;
+  base.X = plan->X;
+  base.batch = B;
+  base.tab_bs = d->tab_bstride;
+  base.tab_real = d->tab_real;
+  base.dxdp = d->dxdp;
+  base.scale_const = 1.0;
+  base.M = M;
+  base.Mx = d->Mx;
+  base.Mp = d->Mp;
+  base.wx_bs = d->wx_bstride;
+  base.wp_bs = d->wp_bstride;
+  base.s0 = d->s0;
+  base.s0_bs = d->s0_bstride;
+  base.blend_c = d->blend_c;
+  base.out_scale = 1.0;
+
+  auto tabV = [&](int k) { return advance(d->tabV, (long long)k * d->tabV_step, tes); };
+  auto tabK = [&](int k) { return advance(d->tabK, (long long)k * d->tabK_step, tes); };
+  auto gV = [&](int k) { return advance(d->gV, (long long)k * d->gV_step, 2 * rs); };
+  auto gK = [&](int k) { return advance(d->gK, (long long)k * d->gK_step, 2 * rs); };
+  auto ring = [&](int k) { return plan->ring + (size_t)(k & 1) * ring_slot; };
+  auto hist = [&](int k) { return d->obs_out == nullptr ? nullptr : d->obs_out + (size_t)k * B * M; };
+
+  auto col = [&](PassArgs a) -> int {
+    a.tw = plan->twP;
+    int np = 0;
+    cudaError_t e = launch_col(a, plan->dtype, st, &np);
+    if (e != cudaSuccess) return cuda_fail(e, "column pass launch");
+    return FW_OK;
+  };
+  auto row = [&](PassArgs a) -> int {
+    a.tw = plan->twX;
+    cudaError_t e = launch_row(a, plan->dtype, st);
+    if (e != cudaSuccess) return cuda_fail(e, "row pass launch");
+    return FW_OK;
+  };
+  auto obs_args = [&](PassArgs& a, int k) {
+    a.part_out = ring(k);
+    a.wx = d->wx == nullptr ? nullptr : d->wx + (size_t)k * d->wx_step;
+    a.wp = d->wp == nullptr ? nullptr : d->wp + (size_t)k * d->wp_step;
+  };
+  auto prev_args = [&](PassArgs& a, int k) {  // normalisation from the partials of step k
+    a.prev_part = ring(k);
+    a.prev_nparts = plan->nparts;
+    a.obs_hist = hist(k);
+  };
+  int rc = FW_OK;
+  if (d->step_kind == FW_STEP_FUSED) {
+    PassArgs a = base;  // opening V/2 of step 0
+    a.tab1 = tabV(0);
+    a.g1 = gV(0);
+    a.scale_const = d->in_scale;
+    if ((rc = col(a)) != FW_OK) return rc;
+    for (int k = 0; k < steps; ++k) {
+      PassArgs r = base;
+      r.tab1 = tabK(k);
+      r.g1 = gK(k);
+      if (k > 0) prev_args(r, k - 1);
+      if ((rc = row(r)) != FW_OK) return rc;
+      PassArgs c = base;
+      c.tab1 = tabV(k);
+      c.g1 = gV(k);
+      c.bxp = d->bxp;
+      c.bxp_bs = d->bxp_bstride;
+      obs_args(c, k);
+      if (k + 1 < steps) {
+        c.tab2 = tabV(k + 1);
+        c.g2 = gV(k + 1);
+      }
+      if ((rc = col(c)) != FW_OK) return rc;
+    }
+  } else {
+    for (int k = 0; k < steps; ++k) {
+      PassArgs c1 = base;
+      c1.tab1 = tabV(k);
+      c1.g1 = gV(k);
+      c1.blend_pre = 1;
+      if (k > 0) prev_args(c1, k - 1);
+      else c1.scale_const = d->in_scale;
+      if ((rc = col(c1)) != FW_OK) return rc;
+      PassArgs r = base;
+      r.tab1 = tabK(k);
+      r.g1 = gK(k);
+      if ((rc = row(r)) != FW_OK) return rc;
+      PassArgs c2 = base;
+      c2.tab1 = tabV(k);
+      c2.g1 = gV(k);
+      c2.bxp = d->bxp;
+      c2.bxp_bs = d->bxp_bstride;
+      c2.blend_post = 1;
+      obs_args(c2, k);
+      if ((rc = col(c2)) != FW_OK) return rc;
+    }
+  }
+  PassArgs f = base;
+  prev_args(f, steps - 1);
+  cudaError_t e = launch_finalize(f, plan->dtype, st);
+  if (e != cudaSuccess) return cuda_fail(e, "finalize launch");
+  return FW_OK;
+}
+
+// ---------------------------------------------------------------------------
+namespace fw {
+template <typename Rl>
+__global__ void weighted_sum_kernel(const Rl* W, long long w_bs, const double* F, size_t n, double* part) {
+  const int b = blockIdx.y;
+  const Rl* w = W + (size_t)b * w_bs;
+  double s = 0.0, s2 = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = (double)w[i];
+    s += F ? v * F[i] : v;
+    s2 += v * v;
+  }
+  __shared__ double r1[32], r2[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) { r1[threadIdx.x >> 5] = s; r2[threadIdx.x >> 5] = s2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, c = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += r1[k]; c += r2[k]; }
+    part[((size_t)b * gridDim.x + blockIdx.x) * 2 + 0] = a;
+    part[((size_t)b * gridDim.x + blockIdx.x) * 2 + 1] = c;
+  }
+}
+__global__ void sum_parts_kernel(const double* part, int nparts, double* out) {
+  const int b = blockIdx.x;
+  if (threadIdx.x < 2) {
+    double a = 0;
+    for (int k = 0; k < nparts; ++k) a += part[((size_t)b * nparts + k) * 2 + threadIdx.x];
+    out[b * 2 + threadIdx.x] = a;
+  }
+}
+}  // namespace fw
+
+extern "C" int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long long w_bstride, const double* F,
+                                      double* out, void* stream) {
+  if (plan == nullptr || W == nullptr || out == nullptr) return fail(FW_EINVAL, "fw_wigner_weighted_sum: NULL argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t n = (size_t)plan->P * plan->X;
+  dim3 grid(plan->wsum_blocks, plan->batch);
+  if (plan->dtype == FW_F32)
+    weighted_sum_kernel<float><<<grid, 256, 0, st>>>(static_cast<const float*>(W), w_bstride, F, n, plan->wsum);
+  else
+    weighted_sum_kernel<double><<<grid, 256, 0, st>>>(static_cast<const double*>(W), w_bstride, F, n, plan->wsum);
+  sum_parts_kernel<<<plan->batch, 32, 0, st>>>(plan->wsum, plan->wsum_blocks, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "weighted sum launch");
+  return FW_OK;
+}

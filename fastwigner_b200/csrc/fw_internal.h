@@ -1,0 +1,18 @@
+// Internal declarations shared by the CUDA translation units of libfastwigner.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "../../include/fastwigner.h"
+
+namespace fw {
+struct PassArgs;
+cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st);
+cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* nparts);
+cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st);
+int col_parts(int dtype, int P, int X);
+bool size_supported(int n);
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+}  // namespace fw

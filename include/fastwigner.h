@@ -1,0 +1,138 @@
+/*
+ * fastwigner.h -- C ABI of libfastwigner (B200 / sm_100a split-operator
+ * propagators for phase-space quantum dynamics).
+ *
+ * Plain C: opaque handles, raw device pointers, sizes and an int status
+ * (0 = success; otherwise fw_last_error() holds a message).  Device pointers
+ * are caller-owned (the Python layer passes torch CUDA tensor storage); the
+ * library owns only its plan scratch (twiddle tables, partial-sum rings).
+ * All work is enqueued on the caller's stream (cudaStream_t passed as void*,
+ * NULL = legacy default stream).  A handle must not be used from two host
+ * threads at once.
+ *
+ * Reference interfaces replaced (dibondar/FastWigner, paths within that project):
+ *   - cuFFT ctypes binding + plans  cufft.py:105-342
+ *   - WignerMoyalCUDA1D.single_step_propagation / propagate
+ *                                   wigner_moyal_cuda_1d.py:496-540
+ *   - WignerMoyalFTTW1D.single_step_propagation / propagate
+ *                                   wigner_moyal_fftw_1d.py:397-440
+ *   - WignerBlochCUDA1D.bloch_single_step_propagation
+ *                                   wigner_bloch_cuda_1d.py:229-254
+ *   - WignerRandomCollisionModelFFTW1D.single_step_propagation
+ *                                   wigner_random_collision_model_fftw_1d.py:56-76
+ */
+#ifndef FASTWIGNER_H
+#define FASTWIGNER_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FW_ABI_VERSION 1
+
+/* element types of the state buffers */
+#define FW_F32 0 /* float state, complex64 spectra (FP64 phase arguments) */
+#define FW_F64 1 /* double state, complex128 spectra */
+
+/* status codes */
+#define FW_OK 0
+#define FW_EINVAL 1   /* bad argument (size, null pointer, unsupported grid) */
+#define FW_ECUDA 2    /* a CUDA runtime call failed */
+#define FW_ENVRTC 3   /* run-time compilation of a user expression failed */
+#define FW_ESTATE 4   /* handle in the wrong state */
+
+/* step structure of fw_wigner_propagate */
+#define FW_STEP_FUSED 0 /* V/2 K V/2 with the closing V/2 of step n fused with the
+                           opening V/2 of step n+1 (Moyal, Bloch): 2 passes/step */
+#define FW_STEP_SPLIT 1 /* blend V/2 K V/2 blend (random-collision model): 3 passes/step */
+
+/* Library version of this header; fw_abi_version() must return it. */
+int fw_abi_version(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* fw_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Wigner-function (real P x X grid) split-operator plans                    */
+/* ------------------------------------------------------------------------ */
+
+typedef struct fw_wigner_plan fw_wigner_plan;
+
+/*
+ * Create a plan for `batch` Wigner functions of P x X points (p rows, x
+ * fastest) in precision `dtype` (FW_F32 / FW_F64).  P and X must be powers of
+ * two in [128, 4096].  Replaces the four cuFFT D2Z/Z2D axis plans and the
+ * aliased theta-x / p-lambda buffers of WignerMoyalCUDA1D.__init__
+ * (wigner_moyal_cuda_1d.py:285-339, cufft.py:160-213) and the pyFFTW plans of
+ * WignerMoyalFTTW1D.__init__ (wigner_moyal_fftw_1d.py:303-366): the spectra
+ * never leave the chip, so no spectrum buffer exists.
+ */
+int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wigner_plan** out);
+int fw_wigner_plan_destroy(fw_wigner_plan* plan);
+
+/* Number of per-step observables (M) the plan writes for Mx x-weights and Mp p-weights: 2 + Mx + Mp.
+ * Observable slots per instance and step: [sum W, sum W^2, sum W*wx_0(x) .., sum W*wp_0(p) ..]
+ * (sums over the grid of the un-normalised state; ratios give normalised averages). */
+int fw_wigner_num_obs(int Mx, int Mp);
+
+typedef struct fw_wigner_desc {
+  void* W;                  /* device state, batch x P x X */
+  long long w_bstride;      /* elements between instances */
+  int step_kind;            /* FW_STEP_FUSED or FW_STEP_SPLIT */
+  /* phase tables, device; complex (re,im interleaved) unless tab_real:
+     tabV: (P/2+1) x X half spectrum over (theta, x); tabK: P x (X/2+1) over (p, lambda).
+     Table for step k is base + k * *_step elements; tab_bstride between instances. */
+  const void* tabV;
+  long long tabV_step;
+  const void* tabK;
+  long long tabK_step;
+  long long tab_bstride;
+  int tab_real;             /* 1: real exponent tables (Bloch) */
+  /* optional separable per-step factors, complex, gV: P/2+1 over theta, gK: X/2+1 over lambda */
+  const void* gV;
+  long long gV_step;
+  const void* gK;
+  long long gK_step;
+  /* optional real P x X multiplier applied after every step (abs_boundary_x_p) */
+  const void* bxp;
+  long long bxp_bstride;
+  /* FW_STEP_SPLIT: W <- blend_c * W + s0 before and after every step */
+  const void* s0;
+  long long s0_bstride;
+  double blend_c;
+  /* observables: Mx x-weights (Mx x X doubles), Mp p-weights (Mp x P doubles); Mx, Mp <= 4 */
+  int Mx;
+  int Mp;
+  const double* wx;
+  long long wx_step;
+  long long wx_bstride;
+  const double* wp;
+  long long wp_step;
+  long long wp_bstride;
+  double* obs_out;          /* device, steps x batch x M doubles (may be NULL: no history kept) */
+  double dxdp;              /* phase-space cell, for the normalisation sum(W) dX dP = 1 */
+  double in_scale;          /* factor applied to W on the first load (1.0) */
+} fw_wigner_desc;
+
+/*
+ * Advance every instance by `steps` split-operator steps, renormalising after
+ * each step and recording the per-step observable sums in obs_out.  All work
+ * is enqueued on `stream`; no host synchronisation.  Replaces propagate()
+ * of wigner_moyal_cuda_1d.py:521-540 / wigner_moyal_fftw_1d.py:418-440 and the
+ * Bloch step loop of wigner_bloch_cuda_1d.py:129-165.
+ */
+int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* desc, int steps, void* stream);
+
+/*
+ * out[b*2+0] = sum_{p,x} W[b] * F (F = NULL means F = 1), out[b*2+1] = sum W^2, in FP64.
+ * F is a device P x X double array shared by the batch.  Replaces the
+ * weighted_func kernel + gpuarray.sum of get_average and the gpuarray.dot of
+ * get_purity (wigner_moyal_cuda_1d.py:378-403).  `out` is device memory.
+ */
+int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long long w_bstride, const double* F, double* out,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTWIGNER_H */

@@ -1,0 +1,146 @@
+"""GPU parity of the Wigner-function drop-ins against the reference fixtures
+and the FP64 oracle.
+
+Tolerances: FP64 runs 1e-10 relative (L2 of W and every observable).
+FP32 runs (complex64 spectra, FP64-built phases): 1e-5 relative L2 of W;
+per observable (rtol, atol) from FP32_OBS_TOL.  <x>, <p> and the Ehrenfest
+right-hand sides are held to 1e-5; <H> to 5e-4 relative, because the FP32
+round-off floor of W in the far tails is weighted by V(x) there (V(+-10) = 400
+for the double well): an exact complex64 numpy pipeline shows 6e-5 on the same
+case, the kernels 1.1e-4."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT / "tests" / "golden"))
+from cases import CASES, CONFIG1  # noqa: E402
+
+from oracle.wigner_oracle import WignerOracle, exact_harmonic_gibbs  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+GOLD = ROOT / "tests" / "golden"
+OBS = ("X_average", "P_average", "X_average_RHS", "P_average_RHS", "hamiltonian_average")
+FP64_TOL = 1e-10
+FP32_TOL = 1e-5
+FP32_OBS_TOL = {
+    "X_average": (1e-5, 1e-5),
+    "P_average": (1e-5, 1e-5),
+    "X_average_RHS": (1e-5, 1e-5),
+    "P_average_RHS": (1e-5, 1e-5),
+    "hamiltonian_average": (5e-4, 1e-5),
+}
+
+
+def fw():
+    import fastwigner_b200
+
+    return fastwigner_b200
+
+
+def build(case, precision):
+    cls = getattr(fw(), case["cls"])
+    return cls(**case["kw"], precision=precision)
+
+
+def run(case, precision):
+    obj = build(case, precision)
+    if case["cls"] == "WignerBlochFFTW1D":
+        return obj, obj.get_gibbs_state()
+    obj.set_wignerfunction(case["init"])
+    return obj, obj.propagate(case["steps"])
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_matches_reference_fixture(name):
+    g = np.load(GOLD / f"{name}.npz")
+    obj, W = run(CASES[name], "float64")
+    assert rel_l2(W, g["W"]) < FP64_TOL
+    for k in OBS:
+        if k in g:
+            np.testing.assert_allclose(getattr(obj, k), g[k], rtol=FP64_TOL, atol=1e-13)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp32_matches_reference_fixture(name):
+    g = np.load(GOLD / f"{name}.npz")
+    obj, W = run(CASES[name], "float32")
+    assert rel_l2(W, g["W"]) < FP32_TOL
+    for k in OBS:
+        if k in g:
+            rtol, atol = FP32_OBS_TOL[k]
+            np.testing.assert_allclose(getattr(obj, k), g[k], rtol=rtol, atol=atol)
+
+
+def test_config1_fp64_1000_steps():
+    g = np.load(GOLD / "config1_moyal_256.npz")
+    obj, W = run(CONFIG1, "float64")
+    for k in OBS:
+        np.testing.assert_allclose(getattr(obj, k), g[k], rtol=FP64_TOL, atol=1e-13)
+    np.testing.assert_allclose(np.sum(W ** 2), g["W_sum_sq"], rtol=FP64_TOL)
+    np.testing.assert_allclose(W.sum(axis=0), g["W_col_sums"], rtol=1e-9, atol=1e-13)
+
+
+def test_propagate_in_chunks_equals_one_call():
+    case = CASES["moyal_harmonic_128"]
+    a, Wa = run(case, "float64")
+    b = build(case, "float64")
+    b.set_wignerfunction(case["init"])
+    for _ in range(case["steps"] // 5):
+        Wb = b.propagate(5)
+    assert rel_l2(Wb, Wa) < 1e-13
+    np.testing.assert_allclose(b.X_average, a.X_average, rtol=1e-13)
+
+
+def test_single_step_is_unnormalised_step():
+    case = CASES["moyal_dw_alpha_128x256"]
+    obj = build(case, "float64")
+    obj.set_wignerfunction(case["init"])
+    o = WignerOracle(**{k: v for k, v in case["kw"].items() if k not in ("V", "K", "diff_V", "diff_K")},
+                     V=lambda x: case["kw"]["V"](None, x), K=lambda p: case["kw"]["K"](None, p))
+    o.set_wignerfunction(obj.wignerfunction)
+    o.t += o.dt  # the reference evaluates the exponents at the (incremented) current time
+    obj.t += obj.dt
+    o.single_step()
+    W = obj.single_step_propagation()
+    assert rel_l2(W, o.W) < 1e-12
+
+
+def test_purity_average_sigma():
+    case = CASES["moyal_harmonic_128"]
+    obj, W = run(case, "float64")
+    o = WignerOracle(**{k: v for k, v in case["kw"].items() if k not in ("V", "K", "diff_V", "diff_K")},
+                     V=lambda x: 0.5 * x ** 2, K=lambda p: 0.5 * p ** 2)
+    o.set_wignerfunction(W)
+    assert abs(obj.get_purity() - o.get_purity()) < 1e-12
+    assert abs(obj.get_average(lambda self, x, p: x * p) - o.get_average(lambda x, p: x * p)) < 1e-12
+    # coherent state of the harmonic oscillator: sigma_x sigma_p = 1/2
+    assert abs(obj.get_sigma_x_sigma_p() - 0.5) < 1e-6
+
+
+def test_bloch_fftw_matches_exact_gibbs_at_half_temperature():
+    case = CASES["bloch_fftw_harmonic_128"]
+    obj, W = run(case, "float64")
+    kT = case["kw"]["kT"]
+    err = np.abs(exact_harmonic_gibbs(1.0, kT / 2, obj.X, obj.P) - W).max() * obj.dXdP
+    assert err < 1e-7
+
+
+def test_errors_like_reference():
+    kw = dict(CASES["moyal_harmonic_128"]["kw"])
+    with pytest.raises(AssertionError):
+        fw().WignerMoyalFTTW1D(**{**kw, "X_gridDIM": 127})
+    kw.pop("dt")
+    with pytest.raises(AttributeError):
+        fw().WignerMoyalFTTW1D(**kw)
+    obj = build(CASES["moyal_harmonic_128"], "float64")
+    with pytest.raises(AssertionError):
+        obj.set_wignerfunction(np.zeros((4, 4)))
+    with pytest.raises(NotImplementedError):
+        obj.set_wignerfunction("not a function")
