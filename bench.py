@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark of the fused split-operator Moyal step (FP32 state, complex64
+spectra, FP64-built phases) on the 1024 x 1024 anharmonic double-well
+workload: V = 0.05 x^4 - x^2, K = p^2/2, X_amplitude = P_amplitude = 10,
+dt = 0.005; every instance starts from a Gaussian wave packet with
+x0 ~ U(-2, 2), p0 ~ U(-1, 1), width 0.5 (seeded).  A batch of instances is
+advanced together so the states (B x 4 MiB) exceed the 126 MB L2: every pass
+streams its tile from HBM.
+
+One bench step = one time step of every instance of the batch (two fused
+passes per instance).  value = grid-point steps per second over all ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank advances its own batch (different seeds,
+no data-path collective): weak scaling, time = max over ranks.
+``--impl reference`` times the reference algorithm's CPU path (the FP64
+numpy restatement in oracle/, multi-threaded FFTs) on this host instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GRID = 1024
+AMP = 10.0
+DT = 0.005
+WIDTH = 0.5
+BATCH = 64
+E2E_STEPS = 100
+METRIC = "grid-point steps/sec"
+UNIT = "grid-pt*steps/s"
+BYTES_PER_PT_PASS = 8  # FP32 state read + write per pass (algorithmic)
+
+
+def V(x):
+    return 0.05 * x ** 4 - x ** 2
+
+
+def K(p):
+    return 0.5 * p ** 2
+
+
+def dV(x):
+    return 0.2 * x ** 3 - 2.0 * x
+
+
+def dK(p):
+    return p
+
+
+def initial_states(rng, batch, X, P):
+    """Wigner functions of Gaussian wave packets psi ~ exp(-(x-x0)^2/(2w^2) + i p0 x)."""
+    x0 = rng.uniform(-2.0, 2.0, size=batch)
+    p0 = rng.uniform(-1.0, 1.0, size=batch)
+    out = np.empty((batch, P.shape[0], X.shape[1]), dtype=np.float32)
+    for b in range(batch):
+        out[b] = (np.exp(-((X - x0[b]) ** 2) / WIDTH ** 2 - WIDTH ** 2 * (P - p0[b]) ** 2) / np.pi).astype(np.float32)
+    return out
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [c.strip() for c in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_gbs():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per grid point per column-pass launch from the committed ncu
+    summary (profiles/col_pass_f32_1024.md, line 'dram_bytes_per_point: <v>')."""
+    f = ROOT / "profiles" / "col_pass_f32_1024.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.strip().startswith("dram_bytes_per_point:"):
+            try:
+                return float(ln.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(target_s, steps=None, grid=GRID):
+    """Time the FP64 oracle port (the reference algorithm, multi-threaded FFTs)
+    on one instance; returns (pt-steps/s, steps run, seconds, cores)."""
+    from oracle.wigner_oracle import WignerOracle
+
+    cores = os.cpu_count() or 1
+    o = WignerOracle(X_gridDIM=grid, X_amplitude=AMP, P_gridDIM=grid, P_amplitude=AMP, dt=DT,
+                     V=V, K=K, diff_V=dV, diff_K=dK, fft_workers=cores)
+    o.cache_exponents()
+    rng = np.random.default_rng(12345)
+    o.set_wignerfunction(initial_states(rng, 1, o.X, o.P)[0].astype(np.float64))
+    o.propagate(2)  # warm-up (plans, page faults)
+    if steps is None:
+        t0 = time.perf_counter()
+        o.propagate(3)
+        per = (time.perf_counter() - t0) / 3
+        steps = max(3, int(target_s / per))
+    t0 = time.perf_counter()
+    o.propagate(steps)
+    el = time.perf_counter() - t0
+    return grid * grid * steps / el, steps, el, cores
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    from oracle.wigner_oracle import WignerOracle
+
+    o = WignerOracle(X_gridDIM=GRID, X_amplitude=AMP, P_gridDIM=GRID, P_amplitude=AMP, dt=DT,
+                     V=V, K=K, diff_V=dV, diff_K=dK, fft_workers=cores)
+    o.cache_exponents()
+    rng = np.random.default_rng(12345)
+    o.set_wignerfunction(initial_states(rng, 1, o.X, o.P)[0].astype(np.float64))
+    o.propagate(args.warmup)
+    t0 = time.perf_counter()
+    o.propagate(args.steps)
+    el = time.perf_counter() - t0
+    value = GRID * GRID * args.steps / el
+    sample = f"1 instance of the {GRID}x{GRID} workload, {args.steps} FP64 steps, scipy.fft workers={cores}"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"moyal_double_well_{GRID}x{GRID}", "grid": [GRID, GRID], "dt": DT,
+                   "instances_per_step": 1, "implementation": "FP64 numpy restatement of WignerMoyalFTTW1D"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from fastwigner_b200 import _lib
+    from fastwigner_b200.batch import WignerMoyalBatch
+
+    B = args.batch
+    sim = WignerMoyalBatch(batch=B, X_gridDIM=GRID, X_amplitude=AMP, P_gridDIM=GRID, P_amplitude=AMP, dt=DT,
+                           V=V, K=K, diff_V=dV, diff_K=dK, precision="float32")
+    rng = np.random.default_rng(1000 + rank)
+    W0 = initial_states(rng, B, sim.X, sim.P)
+    W0_pinned = torch.from_numpy(W0).pin_memory()
+    sim.set_wignerfunctions(W0_pinned.cuda())
+    lib = _lib.load()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    obs = torch.empty((max(args.steps, E2E_STEPS), B, 8), dtype=torch.float64, device="cuda")
+    sim.propagate(args.warmup, obs=obs[: args.warmup])
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps of all instances, inputs resident in HBM -------
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    n0 = lib.fw_launch_count()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        sim.propagate(args.steps, obs=obs[: args.steps])
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    launches = lib.fw_launch_count() - n0
+    el_ms = max_over_ranks(start.elapsed_time(end))
+    pts = GRID * GRID * B
+    value = pts * args.steps * world / (el_ms * 1e-3)
+    # sanity: the states stay normalised and finite
+    o = obs[args.steps - 1].cpu().numpy()
+    finite = bool(np.isfinite(o).all())
+
+    # ---- per-kernel timing (CUDA events between launches on the same stream) ---
+    _, ms, kind = sim.propagate_timed(min(50, args.steps))
+    col = ms[kind == 0][1:]  # skip the opening half-step launch
+    row = ms[kind == 1]
+    col_ms, row_ms = float(np.mean(col)), float(np.mean(row))
+    dom_kind, dom_ms = ("column pass (FFT_p, exp(V), iFFT_p, observables, FFT_p, exp(V), iFFT_p)", col_ms) \
+        if col.sum() >= row.sum() else ("row pass (FFT_x, exp(K), iFFT_x)", row_ms)
+    peak, peak_kind = measured_peak_gbs()
+    alg_bytes = BYTES_PER_PT_PASS * pts
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
+    tpp = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tpp * pts) if tpp is not None else None,
+                "kernel": dom_kind, "kernel_ms": dom_ms, "col_ms": col_ms, "row_ms": row_ms,
+                "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs"}
+
+    # ---- end-to-end through the public API: pinned host states in, results out --
+    e2e_calls = max(1, min(5, args.steps // E2E_STEPS))
+    host_out = torch.empty((B, GRID, GRID), dtype=torch.float32).pin_memory()
+    obs_host = torch.empty((E2E_STEPS, B, 8), dtype=torch.float64).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_calls):
+        sim.set_wignerfunctions(W0_pinned.to("cuda", non_blocking=True))
+        ob = sim.propagate(E2E_STEPS, obs=obs[:E2E_STEPS])
+        host_out.copy_(sim.W, non_blocking=True)
+        obs_host.copy_(ob, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = pts * E2E_STEPS * e2e_calls * world / (e2e_ms * 1e-3)
+    h2d = W0_pinned.numel() * 4 / E2E_STEPS
+    d2h = (host_out.numel() * 4 + obs_host.numel() * 8) / E2E_STEPS
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, csteps, cel, cores = cpu_reference_rate(args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"1 instance of the {GRID}x{GRID} workload, {csteps} FP64 steps in {cel:.1f} s "
+                         f"(numpy restatement of WignerMoyalFTTW1D, scipy.fft workers={cores})"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"moyal_double_well_{GRID}x{GRID}_batch{B}", "grid": [GRID, GRID],
+                       "batch_per_gpu": B, "dt": DT, "potential": "0.05 x^4 - x^2", "amplitudes": [AMP, AMP],
+                       "state_bytes_per_gpu": pts * 4, "l2_policy": "inputs larger than L2 (256 MiB states)",
+                       "passes_per_step": 2, "observables_per_step": 8, "finite": finite,
+                       "e2e_call": f"set_wignerfunctions(pinned host) + propagate({E2E_STEPS}) + states and "
+                                   f"observables to pinned host, {e2e_calls} calls"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -52,6 +52,13 @@ _SIGNATURES = [
     ("fw_wigner_num_obs", c_int, [c_int, c_int]),
     ("fw_wigner_propagate", c_int, [c_vp, ctypes.POINTER(WignerDesc), c_int, c_vp]),
     ("fw_wigner_weighted_sum", c_int, [c_vp, c_vp, c_ll, c_vp, c_vp, c_vp]),
+    ("fw_wigner_propagate_timed", c_int, [c_vp, ctypes.POINTER(WignerDesc), c_int, c_vp,
+                                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_int), c_int]),
+    ("fw_launch_count", c_ll, []),
+    ("fw_expr_create", c_int, [ctypes.c_char_p, ctypes.POINTER(c_vp)]),
+    ("fw_expr_destroy", c_int, [c_vp]),
+    ("fw_expr_check", c_int, [ctypes.c_char_p, ctypes.c_char_p, c_int]),
+    ("fw_expr_eval", c_int, [c_vp, ctypes.c_char_p, c_vp, c_ll, c_vp, c_vp, c_vp]),
 ]
 
 _lib = None

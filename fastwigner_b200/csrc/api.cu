@@ -110,6 +110,28 @@ static inline const void* advance(const void* base, long long elems, size_t esz)
   return base == nullptr ? nullptr : static_cast<const char*>(base) + (ptrdiff_t)(elems * (long long)esz);
 }
 
+namespace fw {
+static long long g_launches = 0;
+// optional per-launch timing hook used by fw_wigner_propagate_timed
+struct LaunchTimer {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  cudaStream_t st = nullptr;
+  bool on = false;
+  void mark(int k) {
+    if (!on) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, st);
+    ev.push_back(e);
+    kind.push_back(k);
+  }
+};
+static thread_local LaunchTimer* g_timer = nullptr;
+}  // namespace fw
+
+extern "C" long long fw_launch_count(void) { return g_launches; }
+
 extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d, int steps, void* stream) {
   if (plan == nullptr || d == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate: NULL plan or desc");
   if (steps < 0) return fail(FW_EINVAL, "fw_wigner_propagate: steps must be >= 0");
@@ -160,12 +182,16 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
     int np = 0;
     cudaError_t e = launch_col(a, plan->dtype, st, &np);
     if (e != cudaSuccess) return cuda_fail(e, "column pass launch");
+    ++g_launches;
+    if (g_timer) g_timer->mark(0);
     return FW_OK;
   };
   auto row = [&](PassArgs a) -> int {
     a.tw = plan->twX;
     cudaError_t e = launch_row(a, plan->dtype, st);
     if (e != cudaSuccess) return cuda_fail(e, "row pass launch");
+    ++g_launches;
+    if (g_timer) g_timer->mark(1);
     return FW_OK;
   };
   auto obs_args = [&](PassArgs& a, int k) {
@@ -230,7 +256,33 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   prev_args(f, steps - 1);
   cudaError_t e = launch_finalize(f, plan->dtype, st);
   if (e != cudaSuccess) return cuda_fail(e, "finalize launch");
+  ++g_launches;
+  if (g_timer) g_timer->mark(2);
   return FW_OK;
+}
+
+extern "C" int fw_wigner_propagate_timed(fw_wigner_plan* plan, const fw_wigner_desc* d, int steps, void* stream,
+                                         float* ms_out, int* kind_out, int n_out) {
+  if (ms_out == nullptr || kind_out == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate_timed: NULL output");
+  LaunchTimer t;
+  t.st = static_cast<cudaStream_t>(stream);
+  t.on = true;
+  t.mark(-1);  // start marker
+  g_timer = &t;
+  int rc = fw_wigner_propagate(plan, d, steps, stream);
+  g_timer = nullptr;
+  cudaError_t e = cudaStreamSynchronize(t.st);
+  if (rc == FW_OK && e != cudaSuccess) rc = cuda_fail(e, "fw_wigner_propagate_timed sync");
+  const int n = (int)t.ev.size() - 1;
+  if (rc == FW_OK && n > n_out) rc = fail(FW_EINVAL, "fw_wigner_propagate_timed: output arrays too small");
+  for (int i = 0; rc == FW_OK && i < n; ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t.ev[i], t.ev[i + 1]);
+    ms_out[i] = ms;
+    kind_out[i] = t.kind[i + 1];
+  }
+  for (cudaEvent_t ev : t.ev) cudaEventDestroy(ev);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -280,6 +332,7 @@ extern "C" int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long 
   else
     weighted_sum_kernel<double><<<grid, 256, 0, st>>>(static_cast<const double*>(W), w_bstride, F, n, plan->wsum);
   sum_parts_kernel<<<plan->batch, 32, 0, st>>>(plan->wsum, plan->wsum_blocks, out);
+  g_launches += 2;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "weighted sum launch");
   return FW_OK;

@@ -43,8 +43,8 @@ __device__ __forceinline__ void spectral_mul(cplx_t<Rl> (&v)[RV], const int j, E
 
 // ---------------------------------------------------------------------------
 // Row pass: G groups of T threads, each group owns one pair of rows.
-template <typename Rl, int N, int T, int G>
-__global__ void __launch_bounds__(G* T) row_pass_kernel(PassArgs a) {
+template <typename Rl, int N, int T, int G, int MINB>
+__global__ void __launch_bounds__(G* T, MINB) row_pass_kernel(PassArgs a) {
   using C = cplx_t<Rl>;
   constexpr int RV = N / T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -93,8 +93,8 @@ template <typename Rl> struct Vec2;
 template <> struct Vec2<float> { using type = float2; };
 template <> struct Vec2<double> { using type = double2; };
 
-template <typename Rl, int N, int T, int CP, int S>
-__global__ void __launch_bounds__(CP* T) col_pass_kernel(PassArgs a) {
+template <typename Rl, int N, int T, int CP, int S, int MINB>
+__global__ void __launch_bounds__(CP* T, MINB) col_pass_kernel(PassArgs a) {
   using C = cplx_t<Rl>;
   using V2 = typename Vec2<Rl>::type;
   constexpr int RV = N / T;
@@ -232,40 +232,40 @@ __global__ void finalize_kernel(PassArgs a) {
 template <typename Rl, int N> struct RowCfg;
 template <typename Rl, int N> struct ColCfg;
 // float: T threads per transform, RV = N / T values per thread
-template <> struct RowCfg<float, 128> { static constexpr int T = 16, G = 16; };
-template <> struct RowCfg<float, 256> { static constexpr int T = 32, G = 8; };
-template <> struct RowCfg<float, 512> { static constexpr int T = 32, G = 8; };
-template <> struct RowCfg<float, 1024> { static constexpr int T = 32, G = 8; };
-template <> struct RowCfg<float, 2048> { static constexpr int T = 64, G = 4; };
-template <> struct RowCfg<float, 4096> { static constexpr int T = 128, G = 2; };
-template <> struct RowCfg<double, 128> { static constexpr int T = 16, G = 16; };
-template <> struct RowCfg<double, 256> { static constexpr int T = 16, G = 16; };
-template <> struct RowCfg<double, 512> { static constexpr int T = 32, G = 8; };
-template <> struct RowCfg<double, 1024> { static constexpr int T = 64, G = 4; };
-template <> struct RowCfg<double, 2048> { static constexpr int T = 128, G = 2; };
-template <> struct RowCfg<double, 4096> { static constexpr int T = 256, G = 1; };
+template <> struct RowCfg<float, 128> { static constexpr int T = 16, G = 16, MINB = 1; };
+template <> struct RowCfg<float, 256> { static constexpr int T = 32, G = 4, MINB = 2; };
+template <> struct RowCfg<float, 512> { static constexpr int T = 32, G = 4, MINB = 2; };
+template <> struct RowCfg<float, 1024> { static constexpr int T = 32, G = 4, MINB = 2; };
+template <> struct RowCfg<float, 2048> { static constexpr int T = 64, G = 4, MINB = 1; };
+template <> struct RowCfg<float, 4096> { static constexpr int T = 128, G = 2, MINB = 1; };
+template <> struct RowCfg<double, 128> { static constexpr int T = 16, G = 16, MINB = 1; };
+template <> struct RowCfg<double, 256> { static constexpr int T = 16, G = 16, MINB = 1; };
+template <> struct RowCfg<double, 512> { static constexpr int T = 32, G = 8, MINB = 1; };
+template <> struct RowCfg<double, 1024> { static constexpr int T = 64, G = 4, MINB = 1; };
+template <> struct RowCfg<double, 2048> { static constexpr int T = 128, G = 2, MINB = 1; };
+template <> struct RowCfg<double, 4096> { static constexpr int T = 256, G = 1, MINB = 1; };
 
-template <> struct ColCfg<float, 128> { static constexpr int T = 16, CP = 32; };
-template <> struct ColCfg<float, 256> { static constexpr int T = 32, CP = 16; };
-template <> struct ColCfg<float, 512> { static constexpr int T = 32, CP = 16; };
-template <> struct ColCfg<float, 1024> { static constexpr int T = 32, CP = 16; };
-template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 8; };
-template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 4; };
-template <> struct ColCfg<double, 128> { static constexpr int T = 16, CP = 16; };
-template <> struct ColCfg<double, 256> { static constexpr int T = 16, CP = 16; };
-template <> struct ColCfg<double, 512> { static constexpr int T = 32, CP = 8; };
-template <> struct ColCfg<double, 1024> { static constexpr int T = 64, CP = 8; };
-template <> struct ColCfg<double, 2048> { static constexpr int T = 128, CP = 4; };
-template <> struct ColCfg<double, 4096> { static constexpr int T = 256, CP = 2; };
+template <> struct ColCfg<float, 128> { static constexpr int T = 16, CP = 32, MINB = 1; };
+template <> struct ColCfg<float, 256> { static constexpr int T = 32, CP = 16, MINB = 1; };
+template <> struct ColCfg<float, 512> { static constexpr int T = 32, CP = 16, MINB = 1; };
+template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 8, MINB = 1; };
+template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 8, MINB = 1; };
+template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 4, MINB = 1; };
+template <> struct ColCfg<double, 128> { static constexpr int T = 16, CP = 16, MINB = 1; };
+template <> struct ColCfg<double, 256> { static constexpr int T = 16, CP = 16, MINB = 1; };
+template <> struct ColCfg<double, 512> { static constexpr int T = 32, CP = 8, MINB = 1; };
+template <> struct ColCfg<double, 1024> { static constexpr int T = 64, CP = 8, MINB = 1; };
+template <> struct ColCfg<double, 2048> { static constexpr int T = 128, CP = 4, MINB = 1; };
+template <> struct ColCfg<double, 4096> { static constexpr int T = 256, CP = 2, MINB = 1; };
 
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
 template <typename Rl, int N>
 static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
   using Cfg = RowCfg<Rl, N>;
-  constexpr int T = Cfg::T, G = Cfg::G;
+  constexpr int T = Cfg::T, G = Cfg::G, MINB = Cfg::MINB;
   const size_t smem = (size_t)G * 2 * (N + N / 32) * sizeof(Rl);
-  auto kern = row_pass_kernel<Rl, N, T, G>;
+  auto kern = row_pass_kernel<Rl, N, T, G, MINB>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -280,10 +280,10 @@ static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
 template <typename Rl, int N>
 static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts) {
   using Cfg = ColCfg<Rl, N>;
-  constexpr int T = Cfg::T, CP = Cfg::CP;
+  constexpr int T = Cfg::T, CP = Cfg::CP, MINB = Cfg::MINB;
   constexpr int S = ilog2(N / T > 32 ? 32 : N / T);
   const size_t smem = (size_t)2 * N * CP * sizeof(Rl);
-  auto kern = col_pass_kernel<Rl, N, T, CP, S>;
+  auto kern = col_pass_kernel<Rl, N, T, CP, S, MINB>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

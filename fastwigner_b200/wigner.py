@@ -171,9 +171,11 @@ class _WignerBase:
     def _tables_static(self) -> bool:
         return not (self._v_time_dependent() or self._k_time_dependent())
 
-    def _upload_table(self, a, shape):
+    def _upload_table(self, a, shape, real=None):
         a = np.broadcast_to(a, shape)
-        if getattr(self, "_tab_real", False):
+        if real is None:
+            real = bool(getattr(self, "_tab_real", False))
+        if real:
             return to_device(np.real(a), self._rt, self.device)
         return torch.view_as_real(to_device(a, self._ct, self.device)).contiguous()
 
@@ -226,16 +228,24 @@ class _WignerBase:
         return self._W
 
     # -- propagation ------------------------------------------------------------
-    def _propagate_chunk(self, nsteps, t0, blend=False):
-        """Run nsteps steps starting after time t0; return the observable sums (nsteps x M)."""
+    def _propagate_chunk(self, nsteps, t0, tables=None, weights=None):
+        """Run nsteps steps starting after time t0; return the observable sums (nsteps x M).
+
+        tables: optional (tabV, vstep, tabK, kstep, tab_real) overriding the
+        Hamiltonian's phase tables; weights: optional (wx, wp) overriding the
+        Ehrenfest weights (use (None, None) for none)."""
         times = t0 + self.dt * np.arange(1, nsteps + 1)
-        if self._tables_static():
-            tabV, tabK = self._static_tables()
-            vstep = kstep = 0
+        if tables is not None:
+            tabV, vstep, tabK, kstep, tab_real = tables
         else:
-            tabV, vstep = self._td_tables(times, "V")
-            tabK, kstep = self._td_tables(times, "K")
-        wx, wp = self._obs_weights(times)
+            tab_real = bool(getattr(self, "_tab_real", False))
+            if self._tables_static():
+                tabV, tabK = self._static_tables()
+                vstep = kstep = 0
+            else:
+                tabV, vstep = self._td_tables(times, "V")
+                tabK, kstep = self._td_tables(times, "K")
+        wx, wp = self._obs_weights(times) if weights is None else weights
         Mx = 0 if wx is None else wx.shape[-2]
         Mp = 0 if wp is None else wp.shape[-2]
         M = 2 + Mx + Mp
@@ -247,7 +257,7 @@ class _WignerBase:
         d.tabV, d.tabV_step = ptr(tabV), vstep
         d.tabK, d.tabK_step = ptr(tabK), kstep
         d.tab_bstride = 0
-        d.tab_real = 1 if getattr(self, "_tab_real", False) else 0
+        d.tab_real = 1 if tab_real else 0
         d.bxp = ptr(self._bxp)
         d.s0 = ptr(self._s0)
         d.blend_c = self._blend_c

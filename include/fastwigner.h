@@ -124,6 +124,20 @@ typedef struct fw_wigner_desc {
 int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* desc, int steps, void* stream);
 
 /*
+ * fw_wigner_propagate, additionally timing every kernel launch with CUDA
+ * events on `stream`; blocks until the work is done.  ms_out receives
+ * 2*steps+2 (FW_STEP_FUSED) or 3*steps+1 (FW_STEP_SPLIT) per-launch durations
+ * in milliseconds and kind_out the pass kind of each launch (0 column, 1 row,
+ * 2 finalize).  n_out is the capacity of both arrays.  A profiling helper; no
+ * reference counterpart.
+ */
+int fw_wigner_propagate_timed(fw_wigner_plan* plan, const fw_wigner_desc* desc, int steps, void* stream,
+                              float* ms_out, int* kind_out, int n_out);
+
+/* Number of kernels this library has launched in the process so far. */
+long long fw_launch_count(void);
+
+/*
  * out[b*2+0] = sum_{p,x} W[b] * F (F = NULL means F = 1), out[b*2+1] = sum W^2, in FP64.
  * F is a device P x X double array shared by the batch.  Replaces the
  * weighted_func kernel + gpuarray.sum of get_average and the gpuarray.dot of
@@ -131,6 +145,30 @@ int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* desc, int st
  */
 int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long long w_bstride, const double* F, double* out,
                            void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* User C expressions (NVRTC)                                                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct fw_expr fw_expr;
+
+/*
+ * Compile a CUDA C evaluation module with NVRTC for the current device and
+ * load it.  Every kernel of the module has the C signature
+ *   extern "C" __global__ void name(const double* in, long long n, double* re, double* im)
+ * Replaces PyCUDA SourceModule compilation of the user strings V, K,
+ * boundaries, initial states and observables (wigner_moyal_cuda_1d.py:250-277,
+ * :389-391, :480-483; rho_vneumann_cuda_1d.py:196-204, :325-327, :425-427).
+ */
+int fw_expr_create(const char* source, fw_expr** out);
+int fw_expr_destroy(fw_expr* mod);
+
+/* Compile only (no device needed); the NVRTC log is copied to `log`. */
+int fw_expr_check(const char* source, char* log, int log_len);
+
+/* Launch kernel `name` over n points: in is 10 x n doubles (device), re/im n doubles each (im may be NULL). */
+int fw_expr_eval(fw_expr* mod, const char* name, const double* in, long long n, double* out_re, double* out_im,
+                 void* stream);
 
 #ifdef __cplusplus
 }

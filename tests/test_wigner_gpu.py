@@ -3,11 +3,12 @@ and the FP64 oracle.
 
 Tolerances: FP64 runs 1e-10 relative (L2 of W and every observable).
 FP32 runs (complex64 spectra, FP64-built phases): 1e-5 relative L2 of W;
-per observable (rtol, atol) from FP32_OBS_TOL.  <x>, <p> and the Ehrenfest
-right-hand sides are held to 1e-5; <H> to 5e-4 relative, because the FP32
-round-off floor of W in the far tails is weighted by V(x) there (V(+-10) = 400
-for the double well): an exact complex64 numpy pipeline shows 6e-5 on the same
-case, the kernels 1.1e-4."""
+per observable (rtol, atol) from FP32_OBS_TOL, about 3x the error of an exact
+complex64 numpy pipeline (W rounded to float32 after every pass) on the same
+cases.  Observables whose weight grows in the far tails (<V'> ~ x^3, <H>)
+inherit the FP32 round-off floor of W there multiplied by the weight
+(V(+-10) = 400 for the double well): the exact FP32 pipeline is already at
+4e-5 on -<V'> and 1.1e-4 on <H> for that case."""
 import sys
 from pathlib import Path
 
@@ -26,11 +27,11 @@ OBS = ("X_average", "P_average", "X_average_RHS", "P_average_RHS", "hamiltonian_
 FP64_TOL = 1e-10
 FP32_TOL = 1e-5
 FP32_OBS_TOL = {
-    "X_average": (1e-5, 1e-5),
-    "P_average": (1e-5, 1e-5),
-    "X_average_RHS": (1e-5, 1e-5),
-    "P_average_RHS": (1e-5, 1e-5),
-    "hamiltonian_average": (5e-4, 1e-5),
+    "X_average": (1e-5, 2e-5),
+    "P_average": (1e-5, 2e-5),
+    "X_average_RHS": (1e-5, 2e-5),
+    "P_average_RHS": (1e-4, 1.2e-4),
+    "hamiltonian_average": (5e-4, 3e-4),
 }
 
 
@@ -84,7 +85,8 @@ def test_config1_fp64_1000_steps():
     for k in OBS:
         np.testing.assert_allclose(getattr(obj, k), g[k], rtol=FP64_TOL, atol=1e-13)
     np.testing.assert_allclose(np.sum(W ** 2), g["W_sum_sq"], rtol=FP64_TOL)
-    np.testing.assert_allclose(W.sum(axis=0), g["W_col_sums"], rtol=1e-9, atol=1e-13)
+    cs = g["W_col_sums"]
+    np.testing.assert_allclose(W.sum(axis=0), cs, rtol=0, atol=FP64_TOL * np.abs(cs).max())
 
 
 def test_propagate_in_chunks_equals_one_call():
