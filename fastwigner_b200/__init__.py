@@ -15,6 +15,10 @@ __all__ = [
     "WignerRandomCollisionModelFFTW1D",
 ]
 
+from .rho import RhoBlochCUDA1D, RhoVNeumannCUDA1D
+
+__all__ += ["RhoVNeumannCUDA1D", "RhoBlochCUDA1D"]
+
 try:  # classes that need the NVRTC expression compiler
     from .wigner_cuda import WignerBlochCUDA1D, WignerMoyalCUDA1D  # noqa: F401
 

@@ -43,6 +43,23 @@ class WignerDesc(ctypes.Structure):
     ]
 
 
+class RhoFactor(ctypes.Structure):
+    """Mirror of ``fw_rho_factor``."""
+
+    _fields_ = [("on", c_int), ("s_re", c_dbl), ("s_im", c_dbl), ("u", c_vp), ("w", c_vp), ("tab", c_vp),
+                ("tab_bstride", c_ll), ("shear_c", c_dbl), ("shear_a", c_int), ("shear_b", c_int),
+                ("shear_dx", c_dbl), ("shear_dp", c_dbl), ("sign", c_int)]
+
+
+class RhoDesc(ctypes.Structure):
+    """Mirror of ``fw_rho_desc``."""
+
+    _fields_ = [("R", c_vp), ("r_bstride", c_ll), ("uV", c_vp), ("wV", c_vp), ("V_step", c_ll),
+                ("uK", c_vp), ("wK", c_vp), ("K_step", c_ll), ("bx", c_vp), ("bp", c_vp), ("b_bstride", c_ll),
+                ("Mx", c_int), ("Mp", c_int), ("wx", c_vp), ("wx_step", c_ll), ("gp", c_vp), ("gp_step", c_ll),
+                ("obs_out", c_vp), ("dX", c_dbl)]
+
+
 # (name, restype, argtypes) of every exported entry point
 _SIGNATURES = [
     ("fw_abi_version", c_int, []),
@@ -55,6 +72,12 @@ _SIGNATURES = [
     ("fw_wigner_propagate_timed", c_int, [c_vp, ctypes.POINTER(WignerDesc), c_int, c_vp,
                                           ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_int), c_int]),
     ("fw_launch_count", c_ll, []),
+    ("fw_rho_plan_create", c_int, [c_int, c_int, c_int, ctypes.POINTER(c_vp)]),
+    ("fw_rho_plan_destroy", c_int, [c_vp]),
+    ("fw_rho_num_parts", c_int, [c_vp]),
+    ("fw_rho_pass", c_int, [c_vp, c_vp, c_ll, c_int, ctypes.POINTER(RhoFactor), c_int, ctypes.POINTER(RhoFactor),
+                            ctypes.POINTER(RhoFactor), c_int, ctypes.POINTER(RhoFactor), c_vp, c_vp, c_vp]),
+    ("fw_rho_propagate", c_int, [c_vp, ctypes.POINTER(RhoDesc), c_int, c_vp]),
     ("fw_expr_create", c_int, [ctypes.c_char_p, ctypes.POINTER(c_vp)]),
     ("fw_expr_destroy", c_int, [c_vp]),
     ("fw_expr_check", c_int, [ctypes.c_char_p, ctypes.c_char_p, c_int]),

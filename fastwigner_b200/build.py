@@ -20,7 +20,7 @@ BUILD = PKG / "_build"
 SOURCES = [
     "api.cu",
     "wigner_passes.cu",
-    "rho_passes.cu",
+    "rho_api.cu",
     "expr.cu",
     "fno.cu",
     "batch.cu",

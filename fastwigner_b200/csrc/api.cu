@@ -130,6 +130,7 @@ struct LaunchTimer {
 static thread_local LaunchTimer* g_timer = nullptr;
 }  // namespace fw
 
+void fw::count_launch(long long n) { g_launches += n; }
 extern "C" long long fw_launch_count(void) { return g_launches; }
 
 extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d, int steps, void* stream) {

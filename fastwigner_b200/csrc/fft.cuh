@@ -153,6 +153,8 @@ __device__ __forceinline__ void fft(C (&v)[RV], const int j, EX& ex, const C* __
   stockham<N, T, RV, 1, DIR, C, EX>(v, j, ex, tw);
 }
 
+constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n / 2); }
+
 // Named barrier over `nthreads` threads (multiple of 32) with id 1..15.
 __device__ __forceinline__ void named_barrier(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");

@@ -13,6 +13,7 @@ int col_parts(int dtype, int P, int X);
 bool size_supported(int n);
 
 void set_error(const std::string& msg);
+void count_launch(long long n);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* where);
 }  // namespace fw

@@ -147,6 +147,90 @@ int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long long w_bstr
                            void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Density-matrix plans: rho[b][i][j] = <x'_i| rho |x_j>, complex N x N       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct fw_rho_plan fw_rho_plan;
+
+/*
+ * Plan for `batch` complex N x N density matrices (complex64 for FW_F32,
+ * complex128 for FW_F64), N a power of two in [128, 4096].  Replaces the
+ * cuFFT Z2Z plans of RhoVNeumannCUDA1D (rho_vneumann_cuda_1d.py:212, :238-239;
+ * cufft.py:241-342).
+ */
+int fw_rho_plan_create(int N, int batch, int dtype, fw_rho_plan** out);
+int fw_rho_plan_destroy(fw_rho_plan* plan);
+/* Row-pass partial records per instance (the length of part_out / N for fw_rho_pass). */
+int fw_rho_num_parts(const fw_rho_plan* plan);
+
+/* Element-wise factor f(i, j) = s * u[j] * w[i] * tab[i][j] * exp(i shear_c A(j) B(i)) * (-1)^(i sign),
+ * A, B grid coordinates (0: x = shear_dx (k - N/2), 1: p = shear_dp ((k + N/2) mod N - N/2)). */
+typedef struct fw_rho_factor {
+  int on;
+  double s_re, s_im;
+  const void* u;            /* complex N (state precision), over j; NULL = 1 */
+  const void* w;            /* complex N, over i; NULL = 1 */
+  const void* tab;          /* real N x N (state precision); NULL = 1 */
+  long long tab_bstride;
+  double shear_c;           /* 0: no shear factor */
+  int shear_a, shear_b;
+  double shear_dx, shear_dp;
+  int sign;
+} fw_rho_factor;
+
+/*
+ * One pass over rows (axis 1: transforms along j) or columns (axis 0: along i):
+ * F0 -> T1 -> F1 -> F2 -> T2 -> F3, T = 0 none, -1 forward FFT, +1 unnormalised
+ * inverse FFT.  Row passes may also write per-CTA partials part_out[b][c][4] =
+ * [Re tr, Im tr, sum |rho|^2, 0] of the state after F1, and sum_out[b][c][2] =
+ * complex sum of all elements after F3 (device arrays, fw_rho_num_parts records
+ * per instance).  Replaces the observable, shear and sign-flip kernels with their
+ * axis FFTs (rho_vneumann_cuda_1d.py:431-472, :502-592, :710-800).
+ */
+int fw_rho_pass(fw_rho_plan* plan, void* R, long long r_bstride, int axis, const fw_rho_factor* f0, int t1,
+                const fw_rho_factor* f1, const fw_rho_factor* f2, int t2, const fw_rho_factor* f3, double* part_out,
+                double* sum_out, void* stream);
+
+typedef struct fw_rho_desc {
+  void* R;                  /* device states, batch x N x N complex */
+  long long r_bstride;      /* complex elements between instances */
+  /* exp(V) in the x-representation: factor u[j] w[i] (vN: u = exp(-i dt V(x)/2), w = conj(u);
+     Bloch: u = w = exp(-dbeta (V - V_min/2)/4)); step k uses base + k * V_step complex elements */
+  const void* uV;
+  const void* wV;
+  long long V_step;
+  /* exp(K) in the (fft-ordered) momentum representation, same structure */
+  const void* uK;
+  const void* wK;
+  long long K_step;
+  const void* bx;           /* optional real N x N factor with every exp(V) (abs_boundary_x) */
+  const void* bp;           /* optional real N x N factor with every exp(K) (abs_boundary_p) */
+  long long b_bstride;
+  /* observables: Mx diagonal x-weights (Mx x N doubles) -> Tr[rho f(x)];
+     Mp Toeplitz kernels G = ifft(g(p)) (Mp x N complex doubles) -> Tr[rho g(p)];
+     wx_step and gp_step count doubles */
+  int Mx;
+  int Mp;
+  const double* wx;
+  long long wx_step;
+  const double* gp;
+  long long gp_step;
+  double* obs_out;          /* steps x batch x M doubles, M = 4 + 2 Mx + 2 Mp:
+                               [Re tr, Im tr, sum|rho|^2, 0, (Re, Im) of each x- then p-observable] */
+  double dX;
+} fw_rho_desc;
+
+/*
+ * Advance every density matrix by `steps` split-operator steps
+ * (exp(V) -> FFT2 -> exp(K) -> iFFT2 -> exp(V), then rho /= Tr(rho) dX), two
+ * fused passes per step, observables recorded per step.  Replaces
+ * RhoVNeumannCUDA1D.single_step_propagation / propagate
+ * (rho_vneumann_cuda_1d.py:340-374) and RhoBlochCUDA1D.bloch_single_step_propagation
+ * (rho_bloch_cuda_1d.py:224-241).
+ */
+int fw_rho_propagate(fw_rho_plan* plan, const fw_rho_desc* desc, int steps, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* User C expressions (NVRTC)                                                */
 /* ------------------------------------------------------------------------ */
 
