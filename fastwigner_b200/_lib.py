@@ -72,6 +72,8 @@ _SIGNATURES = [
     ("fw_wigner_propagate_timed", c_int, [c_vp, ctypes.POINTER(WignerDesc), c_int, c_vp,
                                           ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_int), c_int]),
     ("fw_launch_count", c_ll, []),
+    ("fw_wigner_propagate_noalloc", c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(WignerDesc), c_int, c_vp]),
+    ("fw_noalloc_scratch_bytes", ctypes.c_size_t, []),
     ("fw_rho_plan_create", c_int, [c_int, c_int, c_int, ctypes.POINTER(c_vp)]),
     ("fw_rho_plan_destroy", c_int, [c_vp]),
     ("fw_rho_num_parts", c_int, [c_vp]),

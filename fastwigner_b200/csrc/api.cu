@@ -338,3 +338,90 @@ extern "C" int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long 
   if (e != cudaSuccess) return cuda_fail(e, "weighted sum launch");
   return FW_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Propagation without device allocation.
+//
+// Some callers cannot call cudaMalloc: a host program that gives this library
+// only buffers carved from its own fixed device-memory pool (instrument or
+// real-time control loops that size all GPU memory once at start-up), or a
+// loop that must not hit the implicit device-wide synchronisation of
+// cudaMalloc / cudaFree between propagation calls.  For them,
+// fw_wigner_propagate_noalloc runs the same passes as fw_wigner_propagate
+// with the plan scratch (twiddle tables and the partial-sum ring) placed in
+// the fixed array below instead of plan allocations.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB per device, held until process exit
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+constexpr int kMaxDevices = 64;
+static unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+__global__ void noalloc_twiddles_kernel(int n, int dtype, void* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double s, c;
+  sincospi(-2.0 * (double)k / (double)n, &s, &c);
+  if (dtype == FW_F64) {
+    reinterpret_cast<double*>(out)[2 * k] = c;
+    reinterpret_cast<double*>(out)[2 * k + 1] = s;
+  } else {
+    reinterpret_cast<float*>(out)[2 * k] = (float)c;
+    reinterpret_cast<float*>(out)[2 * k + 1] = (float)s;
+  }
+}
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+}  // namespace
+
+extern "C" size_t fw_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, const fw_wigner_desc* desc, int steps,
+                                           void* stream) {
+  if (desc == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: NULL desc");
+  if (dtype != FW_F32 && dtype != FW_F64) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: bad dtype");
+  if (!size_supported(P) || !size_supported(X))
+    return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: P and X must be powers of two in [128, 4096]");
+  if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: batch must be in [1, 65535]");
+  const int np = col_parts(dtype, P, X);
+  if (np <= 0) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: unsupported X for the column pass tile");
+  const size_t rs = dtype == FW_F64 ? sizeof(double) : sizeof(float);
+  const size_t twP_bytes = align256(2 * rs * (size_t)P);
+  const size_t twX_bytes = align256(2 * rs * (size_t)X);
+  const size_t ring_bytes = sizeof(double) * 2 * (size_t)batch * np * MMAX;
+  const size_t need = twP_bytes + twX_bytes + ring_bytes;
+  if (need > kNoAllocScratchBytes)
+    return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: needs " + std::to_string(need) +
+                               " bytes of scratch for this grid and batch, more than the fixed " +
+                               std::to_string(kNoAllocScratchBytes) + " bytes; use fw_wigner_propagate");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: device index too large");
+  if (g_noalloc_ptr[dev] == nullptr) {  // once per device, with that device current
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // every call rewrites the twiddles (earlier calls may have left other sizes);
+  // the partial-sum ring is always written before it is read
+  noalloc_twiddles_kernel<<<(P + 255) / 256, 256, 0, st>>>(P, dtype, base);
+  noalloc_twiddles_kernel<<<(X + 255) / 256, 256, 0, st>>>(X, dtype, base + twP_bytes);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "noalloc twiddle launch");
+  count_launch(2);
+  fw_wigner_plan tmp;
+  tmp.P = P;
+  tmp.X = X;
+  tmp.batch = batch;
+  tmp.dtype = dtype;
+  tmp.nparts = np;
+  tmp.twP = base;
+  tmp.twX = base + twP_bytes;
+  tmp.ring = reinterpret_cast<double*>(base + twP_bytes + twX_bytes);
+  tmp.wsum = nullptr;
+  tmp.wsum_blocks = 0;
+  return fw_wigner_propagate(&tmp, desc, steps, stream);
+}

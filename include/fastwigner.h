@@ -24,6 +24,8 @@
 #ifndef FASTWIGNER_H
 #define FASTWIGNER_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -136,6 +138,29 @@ int fw_wigner_propagate_timed(fw_wigner_plan* plan, const fw_wigner_desc* desc, 
 
 /* Number of kernels this library has launched in the process so far. */
 long long fw_launch_count(void);
+
+/*
+ * fw_wigner_propagate for callers that cannot allocate device memory: no
+ * counterpart in the reference.  Some hosts cannot call cudaMalloc -- a program
+ * that hands this library only buffers from its own fixed device-memory pool
+ * (instrument or real-time control loops that size all GPU memory at start-up),
+ * or a loop that must not hit the device-wide synchronisation of cudaMalloc /
+ * cudaFree between calls.  This entry point takes no plan and allocates
+ * nothing: its scratch (twiddle tables and partial sums) lives in a fixed
+ * array of fw_noalloc_scratch_bytes() (4 MiB) that every GPU loading the
+ * library holds until exit.  Grids and batches needing more scratch
+ * (2*(P+X) reals + 2*batch*(X/(2*CP))*10 doubles) are rejected with
+ * FW_EINVAL.  The first call on a device looks up the array's device address
+ * (make that first call before any stream capture).  All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller.  The caller still owns W, the
+ * tables, weights and obs_out exactly as for fw_wigner_propagate.
+ */
+int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, const fw_wigner_desc* desc, int steps,
+                                void* stream);
+
+/* Size in bytes of the fixed scratch array used by fw_wigner_propagate_noalloc. */
+size_t fw_noalloc_scratch_bytes(void);
 
 /*
  * out[b*2+0] = sum_{p,x} W[b] * F (F = NULL means F = 1), out[b*2+1] = sum W^2, in FP64.

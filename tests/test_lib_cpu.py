@@ -13,7 +13,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def header_symbols():
     text = (ROOT / "include" / "fastwigner.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*|void)\s+\*?(fw_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|size_t|const char\*|void)\s+\*?(fw_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_entry_points():
