@@ -16,8 +16,9 @@ __all__ = [
 ]
 
 from .rho import RhoBlochCUDA1D, RhoVNeumannCUDA1D
+from .strong_field import StrongFieldWigner
 
-__all__ += ["RhoVNeumannCUDA1D", "RhoBlochCUDA1D"]
+__all__ += ["RhoVNeumannCUDA1D", "RhoBlochCUDA1D", "StrongFieldWigner"]
 
 try:  # classes that need the NVRTC expression compiler
     from .wigner_cuda import WignerBlochCUDA1D, WignerMoyalCUDA1D  # noqa: F401

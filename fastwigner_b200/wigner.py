@@ -258,6 +258,11 @@ class _WignerBase:
         d.tabK, d.tabK_step = ptr(tabK), kstep
         d.tab_bstride = 0
         d.tab_real = 1 if tab_real else 0
+        gV, gK = getattr(self, "_gV", None), getattr(self, "_gK", None)
+        if gV is not None:  # separable per-step factors over theta / lambda (complex, steps x len x 2)
+            d.gV, d.gV_step = ptr(gV), gV.shape[-2]
+        if gK is not None:
+            d.gK, d.gK_step = ptr(gK), gK.shape[-2]
         d.bxp = ptr(self._bxp)
         d.s0 = ptr(self._s0)
         d.blend_c = self._blend_c
