@@ -80,6 +80,13 @@ _SIGNATURES = [
     ("fw_rho_pass", c_int, [c_vp, c_vp, c_ll, c_int, ctypes.POINTER(RhoFactor), c_int, ctypes.POINTER(RhoFactor),
                             ctypes.POINTER(RhoFactor), c_int, ctypes.POINTER(RhoFactor), c_vp, c_vp, c_vp]),
     ("fw_rho_propagate", c_int, [c_vp, ctypes.POINTER(RhoDesc), c_int, c_vp]),
+    ("fw_batch_create", c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_int, ctypes.POINTER(c_vp)]),
+    ("fw_batch_destroy", c_int, [c_vp]),
+    ("fw_batch_num_variants", c_int, []),
+    ("fw_batch_set_variant", c_int, [c_vp, c_int]),
+    ("fw_batch_set_instance", c_int, [c_vp, c_int, c_vp, c_vp, c_vp, c_dbl]),
+    ("fw_batch_propagate", c_int, [c_vp, c_int, c_vp, c_int, c_vp]),
+    ("fw_batch_status", c_int, [c_vp, ctypes.POINTER(c_int)]),
     ("fw_expr_create", c_int, [ctypes.c_char_p, ctypes.POINTER(c_vp)]),
     ("fw_expr_destroy", c_int, [c_vp]),
     ("fw_expr_check", c_int, [ctypes.c_char_p, ctypes.c_char_p, c_int]),

@@ -138,3 +138,154 @@ class WignerMoyalBatch:
         self.t += steps * self.dt
         nl = 2 * steps + 2
         return obs, np.array(ms[:nl]), np.array(kind[:nl])
+
+
+# =============================================================================
+# Uneven batches: one persistent launch over instances of different grid sizes
+# =============================================================================
+def _autotune_path():
+    import os
+    from pathlib import Path
+
+    p = os.environ.get("FASTWIGNER_AUTOTUNE")
+    return Path(p) if p else Path.home() / ".cache" / "fastwigner_b200" / "autotune.json"
+
+
+class WignerMoyalUnevenBatch:
+    """Independent FP32 Moyal instances with their own grids (P, X in
+    {128, 256, 512, 1024}), amplitudes and Hamiltonians, advanced by one
+    persistent cooperative launch per ``propagate`` call (optionally replayed
+    as a CUDA graph).  Conventions are WignerMoyalFTTW1D's (static
+    Hamiltonians; exponents as in wigner_moyal_fftw_1d.py:164-213).
+
+    ``specs``: one dict per instance with X_gridDIM, P_gridDIM, X_amplitude,
+    P_amplitude, V (callable of x), K (callable of p).  ``variant`` None picks
+    the launch shape with the autotuner (timings cached in a JSON file keyed by
+    GPU and size mix, the analogue of FFTW wisdom)."""
+
+    def __init__(self, specs, *, dt, t=0.0, hbar=1.0, variant=None, autotune_steps=10):
+        self.dt, self.t, self.hbar = float(dt), float(t), float(hbar)
+        self.device = require_cuda()
+        self._lib = _lib.load()
+        self.specs = [dict(s) for s in specs]
+        n = len(self.specs)
+        P = (ctypes.c_int * n)(*[int(s["P_gridDIM"]) for s in self.specs])
+        X = (ctypes.c_int * n)(*[int(s["X_gridDIM"]) for s in self.specs])
+        self._h = _lib.c_vp()
+        check(self._lib.fw_batch_create(n, P, X, 0, ctypes.byref(self._h)), "fw_batch_create")
+        self.W, self._tabs, self.dXdP = [], [], []
+        for i, s in enumerate(self.specs):
+            Pn, Xn = int(s["P_gridDIM"]), int(s["X_gridDIM"])
+            dX, dP = 2.0 * s["X_amplitude"] / Xn, 2.0 * s["P_amplitude"] / Pn
+            x = np.linspace(-s["X_amplitude"], s["X_amplitude"] - dX, Xn)[None, :]
+            p = np.linspace(-s["P_amplitude"], s["P_amplitude"] - dP, Pn)[:, None]
+            th = np.fft.fftfreq(Pn, dP / (2 * np.pi))[: Pn // 2 + 1][:, None]
+            la = np.fft.fftfreq(Xn, dX / (2 * np.pi))[: Xn // 2 + 1][None, :]
+            h = self.hbar
+            ev = np.broadcast_to(np.exp(-0.5j * self.dt / h * (s["V"](x - 0.5 * h * th) - s["V"](x + 0.5 * h * th))),
+                                 (Pn // 2 + 1, Xn))
+            ek = np.broadcast_to(np.exp(-1j * self.dt / h * (s["K"](p + 0.5 * h * la) - s["K"](p - 0.5 * h * la))),
+                                 (Pn, Xn // 2 + 1))
+            tv = torch.view_as_real(to_device(ev, torch.complex64, self.device)).contiguous()
+            tk = torch.view_as_real(to_device(ek, torch.complex64, self.device)).contiguous()
+            W = torch.zeros((Pn, Xn), dtype=torch.float32, device=self.device)
+            self.W.append(W)
+            self._tabs.append((tv, tk))
+            self.dXdP.append(dX * dP)
+            s.update(X=x, P=p, dX=dX, dP=dP)
+            check(self._lib.fw_batch_set_instance(self._h, i, ptr(W), ptr(tv), ptr(tk), dX * dP),
+                  "fw_batch_set_instance")
+        self.variant = 0
+        if variant is None:
+            variant = self.autotune(autotune_steps)
+        self.set_variant(variant)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.fw_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_variant(self, v):
+        check(self._lib.fw_batch_set_variant(self._h, int(v)), "fw_batch_set_variant")
+        self.variant = int(v)
+
+    def set_wignerfunctions(self, states):
+        """One state per instance (array / tensor of that instance's shape); each is normalised."""
+        for W, s, d in zip(self.W, states, self.dXdP):
+            W.copy_(to_device(s, torch.float32, self.device) if not isinstance(s, torch.Tensor) else s)
+            W.div_(float(W.sum(dtype=torch.float64)) * d)
+        return self
+
+    def propagate(self, steps=1, use_graph=True, obs=None):
+        """Advance every instance; returns the device tensor of per-step sums
+        (steps x ninst x 2: sum W, sum W^2)."""
+        if obs is None:
+            obs = torch.empty((steps, len(self.specs), 2), dtype=torch.float64, device=self.device)
+        check(self._lib.fw_batch_propagate(self._h, int(steps), ptr(obs), 1 if use_graph else 0, stream_handle()),
+              "fw_batch_propagate")
+        self.t += steps * self.dt
+        return obs
+
+    def status(self):
+        st = ctypes.c_int()
+        check(self._lib.fw_batch_status(self._h, ctypes.byref(st)), "fw_batch_status")
+        return st.value
+
+    def purity(self, obs):
+        """2 pi hbar sum(W^2) dXdP of the normalised states, from propagate()'s sums."""
+        o = obs.cpu().numpy() if isinstance(obs, torch.Tensor) else obs
+        d = np.array(self.dXdP)
+        return 2 * np.pi * self.hbar * o[..., 1] / (o[..., 0] ** 2 * d)
+
+    # -- autotuner ----------------------------------------------------------------
+    def _key(self):
+        import collections
+
+        hist = collections.Counter((int(s["P_gridDIM"]), int(s["X_gridDIM"])) for s in self.specs)
+        mix = ",".join(f"{p}x{x}:{c}" for (p, x), c in sorted(hist.items()))
+        return f"{torch.cuda.get_device_name(self.device)}|{mix}"
+
+    def autotune(self, steps=10, cache=True):
+        """Time every launch-shape variant on this batch (states are saved and
+        restored) and return the fastest; results are cached per GPU and size mix."""
+        import json
+
+        path = _autotune_path()
+        key = self._key()
+        if cache and path.exists():
+            try:
+                table = json.loads(path.read_text())
+                if key in table:
+                    return int(table[key]["variant"])
+            except (ValueError, KeyError, OSError):
+                pass
+        saved = [W.clone() for W in self.W]
+        t_saved = self.t
+        times = {}
+        for v in range(self._lib.fw_batch_num_variants()):
+            self.set_variant(v)
+            self.propagate(2, use_graph=False)  # warm-up
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.propagate(steps, use_graph=False)
+            e1.record()
+            torch.cuda.synchronize()
+            times[v] = e0.elapsed_time(e1) / steps
+        for W, s in zip(self.W, saved):
+            W.copy_(s)
+        self.t = t_saved
+        best = min(times, key=times.get)
+        if cache:
+            try:
+                path.parent.mkdir(parents=True, exist_ok=True)
+                table = json.loads(path.read_text()) if path.exists() else {}
+                table[key] = {"variant": best, "ms_per_step": times}
+                path.write_text(json.dumps(table, indent=1))
+            except OSError:
+                pass
+        self.autotune_ms = times
+        return best

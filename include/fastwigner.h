@@ -43,6 +43,9 @@ extern "C" {
 #define FW_ENVRTC 3   /* run-time compilation of a user expression failed */
 #define FW_ESTATE 4   /* handle in the wrong state */
 
+/* device status word of a batched launch (fw_batch_status) */
+#define FW_BATCH_TIMEOUT 1  /* a grid barrier gave up waiting; the launch returned early */
+
 /* step structure of fw_wigner_propagate */
 #define FW_STEP_FUSED 0 /* V/2 K V/2 with the closing V/2 of step n fused with the
                            opening V/2 of step n+1 (Moyal, Bloch): 2 passes/step */
@@ -254,6 +257,38 @@ typedef struct fw_rho_desc {
  * (rho_bloch_cuda_1d.py:224-241).
  */
 int fw_rho_propagate(fw_rho_plan* plan, const fw_rho_desc* desc, int steps, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Persistent batched propagation over instances with uneven grids (FP32)   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct fw_batch fw_batch;
+
+/*
+ * A batch of `ninst` independent FP32 Wigner functions, instance i on a
+ * P[i] x X[i] grid with P, X in {128, 256, 512, 1024}.  fw_batch_propagate
+ * advances all of them with ONE cooperative (persistent) launch: phases of
+ * row / column passes separated by bounded software grid barriers, work items
+ * (instance, tile) pulled from atomic queues and run with the tile code of each
+ * instance's size.  `variant` selects the launch shape (fw_batch_num_variants();
+ * chosen by the Python autotuner).  No reference counterpart (the reference runs
+ * one instance per class, wigner_moyal_cuda_1d.py:521-540).
+ */
+int fw_batch_create(int ninst, const int* P, const int* X, int variant, fw_batch** out);
+int fw_batch_destroy(fw_batch* batch);
+int fw_batch_num_variants(void);
+int fw_batch_set_variant(fw_batch* batch, int variant);
+/* State W (P x X floats), complex64 tables tabV ((P/2+1) x X) and tabK (P x (X/2+1)) of instance i. */
+int fw_batch_set_instance(fw_batch* batch, int i, void* W, const void* tabV, const void* tabK, double dxdp);
+/*
+ * Advance every instance by `steps` steps (Moyal/Bloch split operator with
+ * per-step renormalisation); obs (device, may be NULL) receives steps x ninst x 2
+ * doubles [sum W, sum W^2].  use_graph != 0 replays a CUDA graph of the launch
+ * (captured on first use for this (steps, obs)).
+ */
+int fw_batch_propagate(fw_batch* batch, int steps, double* obs, int use_graph, void* stream);
+/* Synchronous read of the device status word (0 or FW_BATCH_TIMEOUT). */
+int fw_batch_status(fw_batch* batch, int* status_out);
 
 /* ------------------------------------------------------------------------ */
 /* User C expressions (NVRTC)                                                */

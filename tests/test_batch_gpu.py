@@ -1,0 +1,95 @@
+"""Batched propagation: uniform batches (one launch per pass, batch in grid.y)
+and uneven batches (one persistent cooperative launch) against single-instance
+runs and the FP64 oracle."""
+import numpy as np
+import pytest
+
+from oracle.wigner_oracle import WignerOracle
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def dw(a, b):
+    return (lambda x: a * x ** 4 - b * x ** 2), (lambda p: 0.5 * p ** 2)
+
+
+SIZES = [(128, 256), (256, 128), (512, 512), (1024, 256), (128, 128), (256, 1024), (1024, 1024)]
+
+
+def make_specs(rng):
+    specs = []
+    for P, X in SIZES:
+        V, K = dw(rng.uniform(0.02, 0.1), rng.uniform(0.5, 2.0))
+        specs.append(dict(P_gridDIM=P, X_gridDIM=X, X_amplitude=rng.uniform(6, 10), P_amplitude=rng.uniform(6, 10),
+                          V=V, K=K))
+    return specs
+
+
+def initial(s, rng):
+    x0, p0 = rng.uniform(-2, 2), rng.uniform(-1, 1)
+    return (np.exp(-(s["X"] - x0) ** 2 / 0.25 - 0.25 * (s["P"] - p0) ** 2) + 0 * s["X"] * s["P"]).astype(np.float32)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_uneven_batch_matches_oracle(variant):
+    from fastwigner_b200.batch import WignerMoyalUnevenBatch
+
+    rng = np.random.default_rng(3)
+    specs = make_specs(rng)
+    b = WignerMoyalUnevenBatch(specs, dt=0.005, variant=variant)
+    states = [initial(s, rng) for s in b.specs]
+    b.set_wignerfunctions(states)
+    obs = b.propagate(25, use_graph=False)
+    assert b.status() == 0
+    for s, W0, W in zip(b.specs, states, b.W):
+        o = WignerOracle(X_gridDIM=s["X_gridDIM"], X_amplitude=s["X_amplitude"], P_gridDIM=s["P_gridDIM"],
+                         P_amplitude=s["P_amplitude"], dt=0.005, V=s["V"], K=s["K"])
+        o.set_wignerfunction(W0.astype(np.float64))
+        o.propagate(25)
+        assert rel(W.double().cpu().numpy(), o.W) < 1e-5
+    pur = b.purity(obs)
+    assert np.all(np.isfinite(pur)) and np.all(pur <= 1.0 + 1e-4)
+
+
+def test_graph_replay_equals_direct_launch_and_autotune_cache(tmp_path, monkeypatch):
+    from fastwigner_b200.batch import WignerMoyalUnevenBatch
+
+    monkeypatch.setenv("FASTWIGNER_AUTOTUNE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(5)
+    specs = make_specs(rng)
+    a = WignerMoyalUnevenBatch(specs, dt=0.005, variant=None, autotune_steps=3)
+    assert (tmp_path / "tune.json").exists()
+    b = WignerMoyalUnevenBatch(specs, dt=0.005, variant=a.variant)
+    states = [initial(s, rng) for s in a.specs]
+    a.set_wignerfunctions(states)
+    b.set_wignerfunctions(states)
+    for _ in range(3):
+        a.propagate(10, use_graph=True)
+        b.propagate(10, use_graph=False)
+    for Wa, Wb in zip(a.W, b.W):  # same work per item whichever CTA takes it: bit-identical
+        assert np.array_equal(Wa.cpu().numpy(), Wb.cpu().numpy())
+
+
+def test_uniform_batch_equals_single_instances():
+    from fastwigner_b200 import WignerMoyalFTTW1D
+    from fastwigner_b200.batch import WignerMoyalBatch
+
+    V, K = dw(0.05, 1.0)
+    kw = dict(X_gridDIM=256, X_amplitude=10.0, P_gridDIM=256, P_amplitude=10.0, dt=0.005)
+    b = WignerMoyalBatch(batch=3, **kw, V=V, K=K, diff_V=lambda x: 0.2 * x ** 3 - 2 * x, diff_K=lambda p: p,
+                         precision="float64")
+    rng = np.random.default_rng(1)
+    W0 = np.stack([np.exp(-(b.X - rng.uniform(-2, 2)) ** 2 - (b.P - rng.uniform(-1, 1)) ** 2) for _ in range(3)])
+    b.set_wignerfunctions(W0)
+    obs = b.propagate(12).cpu().numpy()
+    for i in range(3):
+        q = WignerMoyalFTTW1D(**kw, t=0.0, V=lambda _, x: V(x), K=lambda _, p: K(p),
+                              diff_V=lambda _, x: 0.2 * x ** 3 - 2 * x, diff_K=lambda _, p: p)
+        q.set_wignerfunction(W0[i])
+        W = q.propagate(12)
+        assert rel(b.W[i].cpu().numpy(), W) < 1e-12
+        np.testing.assert_allclose(obs[:, i, 2] / obs[:, i, 0], q.X_average, rtol=1e-11)
