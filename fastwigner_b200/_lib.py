@@ -87,6 +87,16 @@ _SIGNATURES = [
     ("fw_batch_set_instance", c_int, [c_vp, c_int, c_vp, c_vp, c_vp, c_dbl]),
     ("fw_batch_propagate", c_int, [c_vp, c_int, c_vp, c_int, c_vp]),
     ("fw_batch_status", c_int, [c_vp, ctypes.POINTER(c_int)]),
+    ("fw_fno_sgemm", c_int, [c_int, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_ll, c_ll, c_vp, c_ll, c_ll,
+                              ctypes.c_float, c_vp, c_ll, c_ll, c_int, c_vp]),
+    ("fw_fno_mix", c_int, [c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
+    ("fw_fno_bias_act", c_int, [c_ll, c_int, c_ll, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
+    ("fw_fno_act_bwd", c_int, [c_ll, c_vp, c_vp, c_vp, c_int, c_vp]),
+    ("fw_fno_channel_sum", c_int, [c_int, c_int, c_ll, c_vp, c_vp, c_int, c_vp]),
+    ("fw_fno_rel_l2", c_int, [c_int, c_ll, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    ("fw_fno_adam", c_int, [c_ll, c_vp, c_vp, c_vp, c_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                            ctypes.c_float, c_int, ctypes.c_float, c_vp]),
+    ("fw_fno_features", c_int, [c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fw_expr_create", c_int, [ctypes.c_char_p, ctypes.POINTER(c_vp)]),
     ("fw_expr_destroy", c_int, [c_vp]),
     ("fw_expr_check", c_int, [ctypes.c_char_p, ctypes.c_char_p, c_int]),

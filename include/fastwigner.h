@@ -291,6 +291,37 @@ int fw_batch_propagate(fw_batch* batch, int steps, double* obs, int use_graph, v
 int fw_batch_status(fw_batch* batch, int* status_out);
 
 /* ------------------------------------------------------------------------ */
+/* Fourier-neural-operator surrogate kernels (training and inference, FP32)  */
+/* No reference counterpart: the surrogate seeds the Bloch thermal-state      */
+/* computation (wigner_bloch_cuda_1d.py:129-165).                             */
+/* ------------------------------------------------------------------------ */
+
+/* C[b] = alpha op(A[b]) op(B[b]) + beta C[b]; op(A) M x K, op(B) K x N, row-major,
+ * leading dimensions lda/ldb/ldc, batch strides strideA/B/C (elements), batch <= 65535. */
+int fw_fno_sgemm(int transA, int transB, int M, int N, int K, float alpha, const float* A, long long lda,
+                 long long strideA, const float* B, long long ldb, long long strideB, float beta, float* C,
+                 long long ldc, long long strideC, int batch, void* stream);
+/* Per-mode complex channel mixing, [B][C][2][K] layouts (real block, imaginary block):
+ * mode 0: out = sum_i X[b][i] Y[i][o]; mode 1: out[b][i] = sum_o X[b][o] conj(Y[i][o]);
+ * mode 2: out[i][o] = sum_b conj(X[b][i]) Y[b][o]. */
+int fw_fno_mix(int mode, int B, int Cin, int Cout, int K, const float* X, const float* Y, float* out, void* stream);
+/* pre = X + bias[c] over [B][C][L]; Y = act ? GELU(pre) : pre (pre may be NULL). */
+int fw_fno_bias_act(long long n, int C, long long L, const float* X, const float* bias, float* pre, float* Y, int act,
+                    void* stream);
+/* dpre = act ? dY GELU'(pre) : dY. */
+int fw_fno_act_bwd(long long n, const float* dY, const float* pre, float* dpre, int act, void* stream);
+/* out[c] (+)= sum over b, l of X[b][c][l] (FP64 accumulation). */
+int fw_fno_channel_sum(int B, int C, long long L, const float* X, float* out, int accumulate, void* stream);
+/* loss[b] = |Y_b - T_b|^2 / |T_b|^2 (doubles); dY = d(mean loss)/dY (may be NULL). */
+int fw_fno_rel_l2(int B, long long L, const float* Y, const float* T, float* dY, double* loss, void* stream);
+/* Adam with bias correction for step `step` (>= 1) and decoupled weight decay. */
+int fw_fno_adam(long long n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
+                int step, float weight_decay, void* stream);
+/* Lift input [B][NP+2][G0][G1]: NP per-sample parameters broadcast, then xs[G1], ps[G0]. */
+int fw_fno_features(int B, int NP, int G0, int G1, const float* params, const float* xs, const float* ps, float* out,
+                    void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* User C expressions (NVRTC)                                                */
 /* ------------------------------------------------------------------------ */
 
