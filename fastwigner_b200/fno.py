@@ -433,32 +433,42 @@ class BlochSurrogate:
                 log(ep, float(np.mean(losses[-max(1, N // batch):])))
         return losses
 
-    def predict(self, D, a, beta, grid=None):
-        """Surrogate thermal Wigner function on the full grid (normalised, sum W dXdP = 1)."""
-        X = normalise_params(np.array([[D, a, beta]]))
-        out = self.net.forward(X, self.xs, self.ps, cache=False)[0]
-        out = out / (out.double().sum() * self.s.dX * self.s.dP).float()
-        return out
+    def predict(self, Ds, As, beta, chunk=8):
+        """Surrogate thermal Wigner functions on the full grid for instances
+        (Ds, As) at one beta, each normalised to sum W dXdP = 1; (n, G, G)."""
+        Ds, As = np.atleast_1d(Ds), np.atleast_1d(As)
+        outs = []
+        for c0 in range(0, len(Ds), chunk):
+            X = normalise_params(np.stack([Ds[c0:c0 + chunk], As[c0:c0 + chunk],
+                                           np.full(len(Ds[c0:c0 + chunk]), beta)], axis=1))
+            out = self.net.forward(X, self.xs, self.ps, cache=False)
+            outs.append(out / (out.double().sum(dim=(1, 2), keepdim=True) * self.s.dX * self.s.dP).float())
+        return torch.cat(outs)
 
-    def seeded_gibbs(self, Ds, As, beta, refine_fraction=0.2, min_refine=1.0):
-        """Gibbs states at `beta` for instances (Ds, As): surrogate prediction at
-        beta_s = beta - dbeta_r, then plain Bloch refinement over dbeta_r =
-        max(refine_fraction * beta, min_refine) (capped at beta)."""
+    def refine_split(self, beta, refine_fraction=0.2, min_refine=1.0):
+        """(beta_s, steps): the surrogate predicts beta_s, the plain Bloch
+        refinement runs the remaining steps; beta_s = 0 means no seeding."""
         db = min(beta, max(refine_fraction * beta, min_refine))
         bs = beta - db
-        bb = BlochBatch(self.s, Ds, As)
+        n_total = int(round(beta / self.s.dbeta))
+        if bs <= 0:
+            return 0.0, n_total
+        return bs, n_total - int(round(bs / self.s.dbeta))
+
+    def seeded_gibbs(self, bb: "BlochBatch", Ds, As, beta, refine_fraction=0.2, min_refine=1.0):
+        """Gibbs states at `beta` for the instances of `bb` (tables for (Ds, As)):
+        surrogate prediction at beta_s, then plain Bloch refinement to beta."""
+        bs, n = self.refine_split(beta, refine_fraction, min_refine)
         if bs <= 0:
             bb.set_uniform()
-            n = int(round(beta / self.s.dbeta))
         else:
-            seeds = torch.stack([self.predict(D, a, bs) for D, a in zip(Ds, As)])
-            bb.set_states(seeds)
-            n = int(round(beta / self.s.dbeta)) - int(round(bs / self.s.dbeta))
+            bb.set_states(self.predict(Ds, As, bs))
         bb.run(n)
         return bb.W, n
 
-    def plain_gibbs(self, Ds, As, beta):
-        bb = BlochBatch(self.s, Ds, As).set_uniform()
+    def plain_gibbs(self, bb: "BlochBatch", beta):
+        """The reference path: Bloch steps from W = const (wigner_bloch_cuda_1d.py:129-165)."""
+        bb.set_uniform()
         n = int(round(beta / self.s.dbeta))
         bb.run(n)
         return bb.W, n

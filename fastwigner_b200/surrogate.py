@@ -1,0 +1,91 @@
+"""Train the FNO surrogate on plain-Bloch thermal states and measure what it
+gains: wall time to a thermal state with and without the surrogate seed.
+
+    python -m fastwigner_b200.surrogate [--runs 200] [--epochs 12] [--out results.json]
+
+The workload is the Morse-oscillator thermal-state problem
+(V = D (1 - exp(-a (x - x_e)))^2, D ~ U(2, 10), a ~ U(0.5, 1.5),
+beta ~ logU(0.1, 20), dbeta = 1e-3, 512^2 FP32).  Error is measured with the
+reference's own metric for thermal states, max |W - W_plain| dX dP
+(wigner_bloch_fftw_1d.py:165-167), against the plain Bloch run from W = const
+on the same GPU; both runs are timed with CUDA events.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from .fno import BlochBatch, BlochSurrogate, FNO2d, MorseBlochSetup, generate_dataset
+
+
+def timed(fn):
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def run_study(runs=200, nbeta=100, epochs=12, batch=16, grid=512, train_grid=128, eval_betas=(5.0, 10.0, 20.0),
+              n_eval=16, refine_fraction=0.2, seed=0, width=32, modes=(16, 16), layers=4, log=print):
+    rng = np.random.default_rng(seed)
+    setup = MorseBlochSetup(grid=grid)
+    betas = np.exp(np.linspace(np.log(0.1), np.log(20.0), nbeta))
+    t0 = time.time()
+    P, S = generate_dataset(setup, runs, betas, rng, train_grid=train_grid)
+    t_data = time.time() - t0
+    net = FNO2d(n_params=3, width=width, modes=modes, layers=layers, proj=128, seed=seed)
+    sur = BlochSurrogate(setup, net, train_grid=train_grid)
+    t0 = time.time()
+    losses = sur.train(P, S, epochs=epochs, batch=batch, rng=rng,
+                       log=(lambda ep, l: log(f"epoch {ep}: loss {l:.3e}")) if log else None)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    dxdp = setup.dX * setup.dP
+    results = []
+    for beta in eval_betas:
+        Ds = rng.uniform(2.0, 10.0, size=n_eval)
+        As = rng.uniform(0.5, 1.5, size=n_eval)
+        bb = BlochBatch(setup, Ds, As)  # exponent tables shared by both runs
+        sur.predict(Ds[:1], As[:1], beta)  # warm-up (DFT matrices for the full grid)
+        bb.set_uniform().run(2)
+        (Wp, n_plain), ms_plain = timed(lambda: sur.plain_gibbs(bb, beta))
+        Wp = Wp.clone()
+        (Ws, n_seed), ms_seed = timed(lambda: sur.seeded_gibbs(bb, Ds, As, beta, refine_fraction=refine_fraction))
+        err = ((Ws - Wp).abs().amax(dim=(1, 2)).double() * dxdp).cpu().numpy()
+        seed_only = sur.predict(Ds, As, beta)
+        err_seed_only = ((seed_only - Wp).abs().amax(dim=(1, 2)).double() * dxdp).cpu().numpy()
+        del bb
+        results.append(dict(beta=beta, instances=n_eval, plain_steps=n_plain, seeded_steps=n_seed,
+                            plain_ms=ms_plain, seeded_ms=ms_seed, speedup=ms_plain / ms_seed,
+                            max_err=float(err.max()), median_err=float(np.median(err)),
+                            surrogate_only_max_err=float(err_seed_only.max())))
+        if log:
+            log(json.dumps(results[-1]))
+    return dict(data_seconds=t_data, train_seconds=t_train, final_loss=float(np.mean(losses[-50:])),
+                samples=int(len(P)), epochs=epochs, results=results)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--runs", type=int, default=200)
+    ap.add_argument("--nbeta", type=int, default=100)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--refine", type=float, default=0.2)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine)
+    print(json.dumps(r))
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(r, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
