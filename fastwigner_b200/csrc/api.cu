@@ -57,6 +57,8 @@ struct fw_wigner_plan {
   double* ring = nullptr;  // 2 x batch x nparts x MMAX partial sums
   double* wsum = nullptr;  // scratch for fw_wigner_weighted_sum partials
   int wsum_blocks = 0;
+  void* wph = nullptr;  // spectra of the p-observable weights (wph_nb x 4 x P complex)
+  int wph_nb = 0;
 };
 
 static constexpr int MMAX = 2 + 8;
@@ -88,6 +90,13 @@ extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wign
     cudaError_t e = cudaMalloc(&p->wsum, sizeof(double) * 2 * (size_t)batch * p->wsum_blocks);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(weighted-sum scratch)");
   }
+  if (rc == FW_OK) {
+    // per-instance weight spectra while they fit in 64 MiB, else shared weights only
+    const size_t per = (size_t)4 * P * 2 * (dtype == FW_F64 ? sizeof(double) : sizeof(float));
+    p->wph_nb = per * (size_t)batch <= ((size_t)64 << 20) ? batch : 1;
+    cudaError_t e = cudaMalloc(&p->wph, per * p->wph_nb);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(weight spectra)");
+  }
   if (rc != FW_OK) {
     fw_wigner_plan_destroy(p);
     return rc;
@@ -102,6 +111,7 @@ extern "C" int fw_wigner_plan_destroy(fw_wigner_plan* p) {
   cudaFree(p->twX);
   cudaFree(p->ring);
   cudaFree(p->wsum);
+  cudaFree(p->wph);
   delete p;
   return FW_OK;
 }
@@ -207,6 +217,24 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   };
   int rc = FW_OK;
   if (d->step_kind == FW_STEP_FUSED) {
+    // The two potential half-steps between kinetic steps share one transform
+    // pair (observables from the mid-point spectrum) unless an x-p mask
+    // (bxp) sits between them, or the p-weights change with the step or do
+    // not fit the plan's spectrum buffer.
+    bool fuse = d->bxp == nullptr;
+    if (fuse && d->Mp > 0) {
+      const int nb = d->wp_bstride != 0 ? B : 1;
+      if (d->wp_step != 0 || plan->wph == nullptr || nb > plan->wph_nb) {
+        fuse = false;
+      } else {
+        base.wph = plan->wph;
+        base.wph_bs = d->wp_bstride != 0 ? 4LL * plan->P : 0;
+        cudaError_t e = launch_pweight_dft(d->wp, d->wp_bstride, d->Mp, plan->P, nb, plan->wph, 4LL * plan->P,
+                                           plan->dtype, st);
+        if (e != cudaSuccess) return cuda_fail(e, "weight spectrum launch");
+        ++g_launches;
+      }
+    }
     PassArgs a = base;  // opening V/2 of step 0
     a.tab1 = tabV(0);
     a.g1 = gV(0);
@@ -227,6 +255,7 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
       if (k + 1 < steps) {
         c.tab2 = tabV(k + 1);
         c.g2 = gV(k + 1);
+        c.fuse_mid = fuse ? 1 : 0;
       }
       if ((rc = col(c)) != FW_OK) return rc;
     }

@@ -122,7 +122,10 @@ __device__ __forceinline__ void do_col(const BatchArgs& a, const BatchInst& in, 
   p.tw = in.twP;
   if (!open) {
     p.part_out = in.part + (size_t)(k & 1) * in.ncol * BM;
-    if (k + 1 < a.steps) p.tab2 = in.tabV;
+    if (k + 1 < a.steps) {
+      p.tab2 = in.tabV;
+      p.fuse_mid = 1;
+    }
   }
   switch (in.P) {
 #define COLN(N_)                                                                                            \

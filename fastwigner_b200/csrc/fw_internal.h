@@ -9,6 +9,8 @@ struct PassArgs;
 cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st);
 cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* nparts);
 cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st);
+cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P, int nb, void* out, long long out_bs,
+                               int dtype, cudaStream_t st);
 int col_parts(int dtype, int P, int X);
 bool size_supported(int n);
 

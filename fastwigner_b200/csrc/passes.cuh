@@ -20,6 +20,12 @@ namespace fw {
 //   tab2:  W  = irfft( rfft(W) * tab2 * g2 ) (second fused half-step; col pass only)
 //   store: W *= out_scale
 //
+// fuse_mid (col pass with tab1 and tab2, no bxp, no blends): the two half-steps
+// share one transform pair, W = irfft( rfft(W) * tab1*g1 * tab2*g2 ), and the
+// partial sums come from the mid-point spectrum (Parseval): sum = DC bin,
+// sum W^2 = |spectrum|^2 / N, sum W wp = Re(spectrum . conj(wph)) / N with
+// wph[q] the forward DFT of wp[q] (wph_bs complex entries between instances).
+//
 // scale_in = scale_const if prev_part == null, else 1/(sum_c prev_part[b][c][0] * dxdp).
 // When obs_hist != null, block 0 of every instance also writes the reduced
 // previous partials (M doubles) to obs_hist[b*M ...].
@@ -56,6 +62,9 @@ struct PassArgs {
   const void* tw;
   double out_scale;
   int* status;  // device status word (error flags); may be null
+  int fuse_mid;
+  const void* wph;  // complex, same precision as W
+  long long wph_bs;
 };
 
 // Reduce previous-pass partial sums (per instance) into the input scale.

@@ -149,4 +149,56 @@ cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Forward DFT Wh[k] = sum_p w[p] exp(-2 pi i k p / P) of each p-observable
+// weight vector, in FP64 (radix-2 Stockham through shared memory, one CTA per
+// vector, twiddles from sincospi of an exact power-of-two ratio), rounded once
+// to the state precision.  Block (q, b): vector q of instance b.
+template <typename Rl>
+__global__ void __launch_bounds__(256) pweight_dft_kernel(const double* wp, long long wp_bs, int P, void* out,
+                                                          long long out_bs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* x = reinterpret_cast<double2*>(smem_raw);
+  double2* y = x + P;
+  const int q = blockIdx.x, b = blockIdx.y;
+  const double* w = wp + (size_t)b * wp_bs + (size_t)q * P;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) x[i] = make_double2(w[i], 0.0);
+  __syncthreads();
+  const int h = P / 2;
+  for (int ns = 1; ns < P; ns <<= 1) {
+    for (int jj = threadIdx.x; jj < h; jj += blockDim.x) {
+      const double2 v0 = x[jj], v1 = x[jj + h];
+      const int k = jj & (ns - 1);
+      double s, c;
+      sincospi(-(double)k / (double)ns, &s, &c);
+      const double tx = v1.x * c - v1.y * s, ty = v1.x * s + v1.y * c;
+      const int d = 2 * (jj - k) + k;
+      y[d] = make_double2(v0.x + tx, v0.y + ty);
+      y[d + ns] = make_double2(v0.x - tx, v0.y - ty);
+    }
+    __syncthreads();
+    double2* t = x;
+    x = y;
+    y = t;
+  }
+  cplx_t<Rl>* o = reinterpret_cast<cplx_t<Rl>*>(out) + (size_t)b * out_bs + (size_t)q * P;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) o[i] = mk<cplx_t<Rl>>((Rl)x[i].x, (Rl)x[i].y);
+}
+
+cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P, int nb, void* out, long long out_bs,
+                               int dtype, cudaStream_t st) {
+  const size_t smem = 2 * sizeof(double2) * (size_t)P;
+  dim3 grid(Mp, nb);
+  cudaError_t e;
+  if (dtype == FW_F32) {
+    e = cudaFuncSetAttribute(pweight_dft_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    pweight_dft_kernel<float><<<grid, 256, smem, st>>>(wp, wp_bs, P, out, out_bs);
+  } else {
+    e = cudaFuncSetAttribute(pweight_dft_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    pweight_dft_kernel<double><<<grid, 256, smem, st>>>(wp, wp_bs, P, out, out_bs);
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace fw

@@ -11,6 +11,25 @@ namespace fw {
 // row and column passes).  v holds the natural-order spectrum Z of a + i b.
 // taba/tabb point at the half-spectrum factors of the two packed sequences;
 // tab_stride is the distance between consecutive half-spectrum entries.
+// Factors of the two packed sequences at full-spectrum index k: table entries
+// kk = min(k, N-k) (taba/tabb, tab_stride apart), times g[kk] when g is given,
+// Hermitian-extended.
+template <typename Rl, int N>
+__device__ __forceinline__ void factor_pair(const void* taba, const void* tabb, size_t tab_stride, int tab_real,
+                                            const void* g, int k, cplx_t<Rl>& ea, cplx_t<Rl>& eb) {
+  using C = cplx_t<Rl>;
+  const int kk = (k <= N / 2) ? k : N - k;
+  ea = tab_load<Rl>(taba, tab_real, (size_t)kk * tab_stride);
+  eb = tab_load<Rl>(tabb, tab_real, (size_t)kk * tab_stride);
+  if (g != nullptr) {
+    const C gk = __ldg(reinterpret_cast<const C*>(g) + kk);
+    ea = cmul(ea, gk);
+    eb = cmul(eb, gk);
+  }
+  ea = herm(ea, k, N);
+  eb = herm(eb, k, N);
+}
+
 template <typename Rl, int N, int T, int RV, typename EX>
 __device__ __forceinline__ void spectral_mul(cplx_t<Rl> (&v)[RV], const int j, EX& ex, const void* taba,
                                              const void* tabb, size_t tab_stride, int tab_real, const void* g,
@@ -22,16 +41,8 @@ __device__ __forceinline__ void spectral_mul(cplx_t<Rl> (&v)[RV], const int j, E
 #pragma unroll
   for (int m = 0; m < RV; ++m) {
     const int k = j + m * T;
-    const int kk = (k <= N / 2) ? k : N - k;
-    C ea = tab_load<Rl>(taba, tab_real, (size_t)kk * tab_stride);
-    C eb = tab_load<Rl>(tabb, tab_real, (size_t)kk * tab_stride);
-    if (g != nullptr) {
-      const C gk = __ldg(reinterpret_cast<const C*>(g) + kk);
-      ea = cmul(ea, gk);
-      eb = cmul(eb, gk);
-    }
-    ea = herm(ea, k, N);
-    eb = herm(eb, k, N);
+    C ea, eb;
+    factor_pair<Rl, N>(taba, tabb, tab_stride, tab_real, g, k, ea, eb);
     const C znk = ex.read((N - k) & (N - 1));
     v[m] = two_real_mul(v[m], znk, ea, eb, f);
   }
@@ -88,6 +99,114 @@ template <typename Rl> struct Vec2;
 template <> struct Vec2<float> { using type = float2; };
 template <> struct Vec2<double> { using type = double2; };
 
+// Reduce the per-thread observable accumulators over the CTA and write the
+// tile's partial-sum record [sum, sum sq, x-obs (Mx), p-obs (Mp)].  Called by
+// every thread of the CTA.
+template <int NTHR>
+__device__ __forceinline__ void obs_store(const PassArgs& a, int b, int tile, int ntiles, double (&acc)[2 + 2 * MAXO],
+                                          double (*ored)[2 + 2 * MAXO]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)  // level-major: the accumulators reduce in parallel
+#pragma unroll
+    for (int q = 0; q < 2 + 2 * MAXO; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int q = 0; q < 2 + 2 * MAXO; ++q) ored[warp][q] = acc[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < a.M) {
+    const int mo = threadIdx.x;
+    const int q = mo < 2 + a.Mx ? mo : 2 + MAXO + (mo - 2 - a.Mx);
+    double t = 0.0;
+    for (int w = 0; w < NTHR / 32; ++w) t += ored[w][q];
+    a.part_out[((size_t)b * ntiles + tile) * a.M + mo] = t;
+  }
+}
+
+// Store a column pair (rows j, j+T, ...) times out_scale.
+template <typename Rl, int N, int T, int RV>
+__device__ __forceinline__ void col_store(const PassArgs& a, const cplx_t<Rl> (&v)[RV], Rl* W, int j, int xa) {
+  using V2 = typename Vec2<Rl>::type;
+  const Rl os = (Rl)a.out_scale;
+  const int X = a.X;
+#pragma unroll
+  for (int m = 0; m < RV; ++m) {
+    const int p = j + m * T;
+    V2 w;
+    w.x = v[m].x * os;
+    w.y = v[m].y * os;
+    *reinterpret_cast<V2*>(W + (size_t)p * X + xa) = w;
+  }
+}
+
+// Mid-point of a fused column pass (a.fuse_mid): v holds the forward spectrum
+// Z of the column pair a + i b (columns xa, xa+1).  Split Z into the two real
+// spectra, apply the closing half-step factors (tab1, g1), take the partial
+// sums from the mid-point spectra, apply the opening factors of the next step
+// (tab2, g2) and repack, scaled for the unnormalised inverse transform.
+//   sum_p a(p)        = A_0
+//   sum_p a(p)^2      = sum_k |A_k|^2 / N
+//   sum_p a(p) w(p)   = sum_k Re(A_k conj(Wh_k)) / N,  Wh = DFT(w)
+template <typename Rl, int N, int T, int RV, typename EX>
+__device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (&v)[RV], const int j, EX& ex,
+                                          int xa, double (&acc)[2 + 2 * MAXO]) {
+  using C = cplx_t<Rl>;
+  const int X = a.X;
+  const size_t esz = a.tab_real ? sizeof(Rl) : sizeof(C);
+  const char* t1 = reinterpret_cast<const char*>(a.tab1) + ((size_t)b * a.tab_bs + xa) * esz;
+  const char* t2 = reinterpret_cast<const char*>(a.tab2) + ((size_t)b * a.tab_bs + xa) * esz;
+  const C* G = reinterpret_cast<const C*>(a.wph) + (size_t)b * a.wph_bs;
+  const bool obs = a.part_out != nullptr;
+  const Rl h = (Rl)(0.5 / (double)N);
+#pragma unroll
+  for (int m = 0; m < RV; ++m) ex.write(j + m * T, v[m]);
+  ex.sync();
+  Rl s2 = 0, ca = 0, cb = 0;
+  Rl sq[MAXO];
+#pragma unroll
+  for (int q = 0; q < MAXO; ++q) sq[q] = 0;
+#pragma unroll
+  for (int m = 0; m < RV; ++m) {
+    const int k = j + m * T;
+    C ea1, eb1, ea2, eb2;
+    factor_pair<Rl, N>(t1, t1 + esz, (size_t)X, a.tab_real, a.g1, k, ea1, eb1);
+    factor_pair<Rl, N>(t2, t2 + esz, (size_t)X, a.tab_real, a.g2, k, ea2, eb2);
+    const C zc = cconj(ex.read((N - k) & (N - 1)));
+    const C A = cmul(cadd(v[m], zc), ea1);   // 2 x spectrum of column a at the mid-point
+    const C Bi = cmul(csub(v[m], zc), eb1);  // 2i x spectrum of column b at the mid-point
+    if (obs) {
+      s2 += A.x * A.x + A.y * A.y + Bi.x * Bi.x + Bi.y * Bi.y;
+      if (m == 0 && j == 0) {  // DC bin: the column sums
+        ca = A.x;
+        cb = Bi.y;
+      }
+      const Rl ur = A.x + Bi.y, ui = A.y - Bi.x;  // 2 x (spectrum a + spectrum b)
+#pragma unroll
+      for (int q = 0; q < MAXO; ++q)
+        if (q < a.Mp) {
+          const C g = __ldg(G + (size_t)q * N + k);
+          sq[q] += ur * g.x + ui * g.y;
+        }
+    }
+    v[m] = cscale(cadd(cmul(A, ea2), cmul(Bi, eb2)), h);
+  }
+  ex.sync();
+  if (obs) {
+    const double da = 0.5 * (double)ca, db = 0.5 * (double)cb;
+    acc[0] = da + db;
+    acc[1] = (double)s2 * (0.25 / (double)N);
+    const double* wx = a.wx + (size_t)b * a.wx_bs;
+#pragma unroll
+    for (int q = 0; q < MAXO; ++q) {
+      acc[2 + q] = (j == 0 && q < a.Mx)
+                       ? da * __ldg(wx + (size_t)q * X + xa) + db * __ldg(wx + (size_t)q * X + xa + 1)
+                       : 0.0;
+      acc[2 + MAXO + q] = (double)sq[q] * (0.5 / (double)N);
+    }
+  }
+}
+
 // One work item of a column pass: instance b, column pairs tile*CP .. tile*CP+CP-1
 // (ntiles = X / (2 CP) tiles per instance, the partial-sum records per instance).
 template <typename Rl, int N, int T, int CP, int S>
@@ -123,6 +242,15 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
       v[m] = mk<C>(bc * v[m].x + w0.x, bc * v[m].y + w0.y);
     }
   }
+  if (a.fuse_mid) {
+    fft<N, T, RV, -1>(v, j, ex, tw);
+    double acc[2 + 2 * MAXO];
+    fused_mid<Rl, N, T, RV>(a, b, v, j, ex, xa, acc);
+    if (a.part_out != nullptr) obs_store<CP * T>(a, b, tile, ntiles, acc, ored);
+    fft<N, T, RV, +1>(v, j, ex, tw);
+    col_store<Rl, N, T, RV>(a, v, W, j, xa);
+    return;
+  }
   const size_t esz = a.tab_real ? sizeof(Rl) : sizeof(C);
   const Rl f = (Rl)(1.0 / (double)N);
   if (a.tab1 != nullptr) {
@@ -157,39 +285,63 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
     double ca = 0.0, cb = 0.0;
     const double* wp = a.wp + (size_t)b * a.wp_bs;
     const int P = N;
+    if constexpr (sizeof(Rl) == 4) {
+      // FP32 state: the 2*CP columns of a row sit in CP adjacent lanes; reduce a
+      // row's sums across them with shuffles, then one lane per row accumulates
+      // the FP64 weighted sums (per-thread column sums over RV rows in FP32).
+      float fa = 0.f, fb = 0.f;
+      constexpr int CH = RV < 8 ? RV : 8;  // rows per batch of independent shuffles
 #pragma unroll
-    for (int m = 0; m < RV; ++m) {
-      const double wa = (double)v[m].x, wb = (double)v[m].y;
-      ca += wa;
-      cb += wb;
-      acc[1] += wa * wa + wb * wb;
-      const int p = j + m * T;
+      for (int m0 = 0; m0 < RV; m0 += CH) {
+        float s[CH], s2[CH];
 #pragma unroll
-      for (int q = 0; q < MAXO; ++q)
-        if (q < a.Mp) acc[2 + MAXO + q] += (wa + wb) * __ldg(wp + (size_t)q * P + p);
+        for (int u = 0; u < CH; ++u) {
+          const float wa = v[m0 + u].x, wb = v[m0 + u].y;
+          fa += wa;
+          fb += wb;
+          s[u] = wa + wb;
+          s2[u] = wa * wa + wb * wb;
+        }
+#pragma unroll
+        for (int o = CP / 2; o >= 1; o >>= 1)
+#pragma unroll
+          for (int u = 0; u < CH; ++u) {  // level-major: CH independent shuffles in flight
+            s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+            s2[u] += __shfl_xor_sync(0xffffffffu, s2[u], o);
+          }
+        if (c == 0) {
+#pragma unroll
+          for (int u = 0; u < CH; ++u) {
+            const int p = j + (m0 + u) * T;
+            acc[0] += (double)s[u];
+            acc[1] += (double)s2[u];
+#pragma unroll
+            for (int q = 0; q < MAXO; ++q)
+              if (q < a.Mp) acc[2 + MAXO + q] += (double)s[u] * __ldg(wp + (size_t)q * P + p);
+          }
+        }
+      }
+      ca = fa;
+      cb = fb;
+    } else {
+#pragma unroll
+      for (int m = 0; m < RV; ++m) {
+        const double wa = (double)v[m].x, wb = (double)v[m].y;
+        ca += wa;
+        cb += wb;
+        acc[1] += wa * wa + wb * wb;
+        const int p = j + m * T;
+#pragma unroll
+        for (int q = 0; q < MAXO; ++q)
+          if (q < a.Mp) acc[2 + MAXO + q] += (wa + wb) * __ldg(wp + (size_t)q * P + p);
+      }
+      acc[0] = ca + cb;
     }
-    acc[0] = ca + cb;
     const double* wx = a.wx + (size_t)b * a.wx_bs;
 #pragma unroll
     for (int q = 0; q < MAXO; ++q)
       if (q < a.Mx) acc[2 + q] = ca * __ldg(wx + (size_t)q * X + xa) + cb * __ldg(wx + (size_t)q * X + xa + 1);
-#pragma unroll
-    for (int q = 0; q < 2 + 2 * MAXO; ++q)
-      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-    const int warp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-      for (int q = 0; q < 2 + 2 * MAXO; ++q) ored[warp][q] = acc[q];
-    }
-    __syncthreads();
-    if (threadIdx.x < a.M) {
-      // output layout: [sum, sum sq, x-obs (Mx), p-obs (Mp)]
-      const int mo = threadIdx.x;
-      const int q = mo < 2 + a.Mx ? mo : 2 + MAXO + (mo - 2 - a.Mx);
-      double t = 0.0;
-      for (int w = 0; w < (CP * T) / 32; ++w) t += ored[w][q];
-      a.part_out[((size_t)b * ntiles + tile) * a.M + mo] = t;
-    }
+    obs_store<CP * T>(a, b, tile, ntiles, acc, ored);
   }
   if (a.tab2 != nullptr) {
     fft<N, T, RV, -1>(v, j, ex, tw);
@@ -197,15 +349,7 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
     spectral_mul<Rl, N, T, RV>(v, j, ex, tb, tb + esz, (size_t)X, a.tab_real, a.g2, f);
     fft<N, T, RV, +1>(v, j, ex, tw);
   }
-  const Rl os = (Rl)a.out_scale;
-#pragma unroll
-  for (int m = 0; m < RV; ++m) {
-    const int p = j + m * T;
-    V2 w;
-    w.x = v[m].x * os;
-    w.y = v[m].y * os;
-    *reinterpret_cast<V2*>(W + (size_t)p * X + xa) = w;
-  }
+  col_store<Rl, N, T, RV>(a, v, W, j, xa);
 }
 
 }  // namespace fw

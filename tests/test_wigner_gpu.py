@@ -146,3 +146,34 @@ def test_errors_like_reference():
         obj.set_wignerfunction(np.zeros((4, 4)))
     with pytest.raises(NotImplementedError):
         obj.set_wignerfunction("not a function")
+
+
+@pytest.mark.parametrize("P", [256, 512, 1024])
+def test_fp32_larger_grids_match_oracle(P):
+    """FP32 parity with the FP64 oracle on the grid sizes of the benchmark workloads."""
+    kw = dict(t=0.0, dt=0.005, X_gridDIM=256, X_amplitude=10.0, P_gridDIM=P, P_amplitude=10.0)
+    V = lambda x: 0.05 * x ** 4 - x ** 2  # noqa: E731
+    init = lambda x, p: np.exp(-(x + 1.3) ** 2 / 0.25 - 0.25 * (p - 0.4) ** 2) + 0 * x * p  # noqa: E731
+    q = fw().WignerMoyalFTTW1D(**kw, V=lambda _, x: V(x), K=lambda _, p: 0.5 * p * p,
+                               diff_V=lambda _, x: 0.2 * x ** 3 - 2 * x, diff_K=lambda _, p: p, precision="float32")
+    q.set_wignerfunction(lambda _, x, p: init(x, p))
+    W = q.propagate(20)
+    o = WignerOracle(**kw, V=V, K=lambda p: 0.5 * p * p, diff_V=lambda x: 0.2 * x ** 3 - 2 * x, diff_K=lambda p: p)
+    o.set_wignerfunction(init(o.X, o.P))
+    o.propagate(20)
+    assert rel_l2(W, o.W) < FP32_TOL
+    for k in ("X_average", "P_average", "X_average_RHS"):
+        rtol, atol = FP32_OBS_TOL[k]
+        np.testing.assert_allclose(getattr(q, k), getattr(o, k), rtol=rtol, atol=atol)
+
+
+def test_fp32_bloch_256():
+    case = dict(CASES["bloch_fftw_harmonic_128"])
+    kw = dict(case["kw"], X_gridDIM=256, P_gridDIM=256)
+    q = fw().WignerBlochFFTW1D(**kw, precision="float32")
+    W = q.get_gibbs_state()
+    o = WignerOracle(**{k: v for k, v in kw.items() if k not in ("kT", "dbeta", "V", "K")},
+                     V=lambda x: 0.5 * x ** 2, K=lambda p: 0.5 * p ** 2)
+    o.setup_bloch_fftw(kw["kT"], kw["dbeta"])
+    o.get_gibbs_state_fftw()
+    assert rel_l2(W, o.W) < FP32_TOL
