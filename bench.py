@@ -272,7 +272,7 @@ def run_ours(args):
     col = ms[kind == 0][1:]  # skip the opening half-step launch
     row = ms[kind == 1]
     col_ms, row_ms = float(np.mean(col)), float(np.mean(row))
-    dom_kind, dom_ms = ("column pass (FFT_p, exp(V), iFFT_p, observables, FFT_p, exp(V), iFFT_p)", col_ms) \
+    dom_kind, dom_ms = ("column pass (FFT_p, exp(V_k) x exp(V_k+1) with observables from the mid-point spectrum, iFFT_p)", col_ms) \
         if col.sum() >= row.sum() else ("row pass (FFT_x, exp(K), iFFT_x)", row_ms)
     peak, peak_kind = measured_peak_gbs()
     alg_bytes = BYTES_PER_PT_PASS * pts

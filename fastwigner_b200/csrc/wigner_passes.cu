@@ -1,9 +1,9 @@
 // Fused half-step passes for real Wigner functions W(x, p) (Moyal, Bloch,
 // random-collision).  A row pass (kinetic step) transforms along x, a column
-// pass (potential step) along p.  Each CTA streams its tile from HBM once,
-// runs forward FFT -> spectral multiply -> inverse FFT (twice for a fused
-// column pass) out of registers and shared memory, and writes the tile back
-// once.  Two real rows/columns are packed into one complex FFT.
+// pass (potential step) along p.  Each CTA streams its tiles from HBM once,
+// runs forward FFT -> spectral multiply -> inverse FFT out of registers and
+// shared memory, and writes each tile back once.  Two real rows/columns are
+// packed into one complex FFT.
 #include "wigner_tiles.cuh"
 #include "fw_internal.h"
 

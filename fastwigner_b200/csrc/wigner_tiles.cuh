@@ -7,10 +7,6 @@
 namespace fw {
 
 // ---------------------------------------------------------------------------
-// spectral multiply between a forward and an inverse transform (shared by the
-// row and column passes).  v holds the natural-order spectrum Z of a + i b.
-// taba/tabb point at the half-spectrum factors of the two packed sequences;
-// tab_stride is the distance between consecutive half-spectrum entries.
 // Factors of the two packed sequences at full-spectrum index k: table entries
 // kk = min(k, N-k) (taba/tabb, tab_stride apart), times g[kk] when g is given,
 // Hermitian-extended.
@@ -30,6 +26,10 @@ __device__ __forceinline__ void factor_pair(const void* taba, const void* tabb, 
   eb = herm(eb, k, N);
 }
 
+// Spectral multiply between a forward and an inverse transform (shared by the
+// row and column passes).  v holds the natural-order spectrum Z of a + i b.
+// taba/tabb point at the half-spectrum factors of the two packed sequences;
+// tab_stride is the distance between consecutive half-spectrum entries.
 template <typename Rl, int N, int T, int RV, typename EX>
 __device__ __forceinline__ void spectral_mul(cplx_t<Rl> (&v)[RV], const int j, EX& ex, const void* taba,
                                              const void* tabb, size_t tab_stride, int tab_real, const void* g,
@@ -140,6 +140,13 @@ __device__ __forceinline__ void col_store(const PassArgs& a, const cplx_t<Rl> (&
   }
 }
 
+// Per-thread partial sums of a fused column pass, in the state precision:
+// sum |2A_k|^2 + |2B_k|^2 over the thread's bins, sum Re(2(A_k+B_k) conj(Wh_k))
+// per p-weight, and (thread j == 0 only) the doubled DC bins of the pair.
+template <typename Rl> struct MidSums {
+  Rl s2, sq[MAXO], ca, cb;
+};
+
 // Mid-point of a fused column pass (a.fuse_mid): v holds the forward spectrum
 // Z of the column pair a + i b (columns xa, xa+1).  Split Z into the two real
 // spectra, apply the closing half-step factors (tab1, g1), take the partial
@@ -150,60 +157,109 @@ __device__ __forceinline__ void col_store(const PassArgs& a, const cplx_t<Rl> (&
 //   sum_p a(p) w(p)   = sum_k Re(A_k conj(Wh_k)) / N,  Wh = DFT(w)
 template <typename Rl, int N, int T, int RV, typename EX>
 __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (&v)[RV], const int j, EX& ex,
-                                          int xa, double (&acc)[2 + 2 * MAXO]) {
+                                          int xa, MidSums<Rl>& o) {
   using C = cplx_t<Rl>;
   const int X = a.X;
   const size_t esz = a.tab_real ? sizeof(Rl) : sizeof(C);
   const char* t1 = reinterpret_cast<const char*>(a.tab1) + ((size_t)b * a.tab_bs + xa) * esz;
   const char* t2 = reinterpret_cast<const char*>(a.tab2) + ((size_t)b * a.tab_bs + xa) * esz;
+  const bool same = a.tab1 == a.tab2 && a.g1 == a.g2;  // time-independent factors: load once
   const C* G = reinterpret_cast<const C*>(a.wph) + (size_t)b * a.wph_bs;
   const bool obs = a.part_out != nullptr;
   const Rl h = (Rl)(0.5 / (double)N);
 #pragma unroll
   for (int m = 0; m < RV; ++m) ex.write(j + m * T, v[m]);
   ex.sync();
-  Rl s2 = 0, ca = 0, cb = 0;
-  Rl sq[MAXO];
+  o.s2 = 0;
+  o.ca = 0;
+  o.cb = 0;
 #pragma unroll
-  for (int q = 0; q < MAXO; ++q) sq[q] = 0;
+  for (int q = 0; q < MAXO; ++q) o.sq[q] = 0;
 #pragma unroll
   for (int m = 0; m < RV; ++m) {
     const int k = j + m * T;
     C ea1, eb1, ea2, eb2;
     factor_pair<Rl, N>(t1, t1 + esz, (size_t)X, a.tab_real, a.g1, k, ea1, eb1);
-    factor_pair<Rl, N>(t2, t2 + esz, (size_t)X, a.tab_real, a.g2, k, ea2, eb2);
+    if (same) {
+      ea2 = ea1;
+      eb2 = eb1;
+    } else {
+      factor_pair<Rl, N>(t2, t2 + esz, (size_t)X, a.tab_real, a.g2, k, ea2, eb2);
+    }
     const C zc = cconj(ex.read((N - k) & (N - 1)));
     const C A = cmul(cadd(v[m], zc), ea1);   // 2 x spectrum of column a at the mid-point
     const C Bi = cmul(csub(v[m], zc), eb1);  // 2i x spectrum of column b at the mid-point
     if (obs) {
-      s2 += A.x * A.x + A.y * A.y + Bi.x * Bi.x + Bi.y * Bi.y;
+      o.s2 += A.x * A.x + A.y * A.y + Bi.x * Bi.x + Bi.y * Bi.y;
       if (m == 0 && j == 0) {  // DC bin: the column sums
-        ca = A.x;
-        cb = Bi.y;
+        o.ca = A.x;
+        o.cb = Bi.y;
       }
       const Rl ur = A.x + Bi.y, ui = A.y - Bi.x;  // 2 x (spectrum a + spectrum b)
 #pragma unroll
       for (int q = 0; q < MAXO; ++q)
         if (q < a.Mp) {
           const C g = __ldg(G + (size_t)q * N + k);
-          sq[q] += ur * g.x + ui * g.y;
+          o.sq[q] += ur * g.x + ui * g.y;
         }
     }
     v[m] = cscale(cadd(cmul(A, ea2), cmul(Bi, eb2)), h);
   }
   ex.sync();
-  if (obs) {
-    const double da = 0.5 * (double)ca, db = 0.5 * (double)cb;
-    acc[0] = da + db;
-    acc[1] = (double)s2 * (0.25 / (double)N);
+}
+
+// Reduce MidSums over the CTA (column-interleaved layout: lane c of a row
+// group is column pair c) and write the tile's partial-sum record.  The bin
+// sums reduce in the state precision within each warp, then in FP64 across
+// warps; the DC terms live in threads j == 0 (tid < CP, all in warp 0).
+template <typename Rl, int N, int CP, int NTHR>
+__device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, int ntiles, MidSums<Rl>& o, int xa,
+                                          double (*ored)[2 + 2 * MAXO]) {
+  static_assert(CP <= 32, "DC lanes must sit in warp 0");
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    o.s2 += __shfl_xor_sync(0xffffffffu, o.s2, off);
+#pragma unroll
+    for (int q = 0; q < MAXO; ++q)
+      if (q < a.Mp) o.sq[q] += __shfl_xor_sync(0xffffffffu, o.sq[q], off);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    ored[warp][1] = (double)o.s2 * (0.25 / (double)N);
+#pragma unroll
+    for (int q = 0; q < MAXO; ++q) ored[warp][2 + MAXO + q] = (double)o.sq[q] * (0.5 / (double)N);
+  }
+  if (warp == 0) {
+    const double da = 0.5 * (double)o.ca, db = 0.5 * (double)o.cb;
+    double d[1 + MAXO];
+    d[0] = da + db;
     const double* wx = a.wx + (size_t)b * a.wx_bs;
 #pragma unroll
-    for (int q = 0; q < MAXO; ++q) {
-      acc[2 + q] = (j == 0 && q < a.Mx)
-                       ? da * __ldg(wx + (size_t)q * X + xa) + db * __ldg(wx + (size_t)q * X + xa + 1)
-                       : 0.0;
-      acc[2 + MAXO + q] = (double)sq[q] * (0.5 / (double)N);
+    for (int q = 0; q < MAXO; ++q)
+      d[1 + q] = (lane < CP && q < a.Mx) ? da * __ldg(wx + (size_t)q * a.X + xa) + db * __ldg(wx + (size_t)q * a.X + xa + 1)
+                                         : 0.0;
+#pragma unroll
+    for (int off = CP / 2; off > 0; off >>= 1)
+#pragma unroll
+      for (int q = 0; q < 1 + MAXO; ++q) d[q] += __shfl_xor_sync(0xffffffffu, d[q], off);
+    if (lane == 0) {
+      ored[0][0] = d[0];
+#pragma unroll
+      for (int q = 0; q < MAXO; ++q) ored[0][2 + q] = d[1 + q];
     }
+  }
+  __syncthreads();
+  if (threadIdx.x < a.M) {
+    const int mo = threadIdx.x;
+    const int q = mo < 2 + a.Mx ? mo : 2 + MAXO + (mo - 2 - a.Mx);
+    double t;
+    if (q == 0 || (q >= 2 && q < 2 + MAXO)) {
+      t = ored[0][q];
+    } else {
+      t = 0.0;
+      for (int w = 0; w < NTHR / 32; ++w) t += ored[w][q];
+    }
+    a.part_out[((size_t)b * ntiles + tile) * a.M + mo] = t;
   }
 }
 
@@ -244,9 +300,9 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
   }
   if (a.fuse_mid) {
     fft<N, T, RV, -1>(v, j, ex, tw);
-    double acc[2 + 2 * MAXO];
-    fused_mid<Rl, N, T, RV>(a, b, v, j, ex, xa, acc);
-    if (a.part_out != nullptr) obs_store<CP * T>(a, b, tile, ntiles, acc, ored);
+    MidSums<Rl> o;
+    fused_mid<Rl, N, T, RV>(a, b, v, j, ex, xa, o);
+    if (a.part_out != nullptr) mid_store<Rl, N, CP, CP * T>(a, b, tile, ntiles, o, xa, ored);
     fft<N, T, RV, +1>(v, j, ex, tw);
     col_store<Rl, N, T, RV>(a, v, W, j, xa);
     return;
