@@ -37,7 +37,9 @@ __global__ void finalize_kernel(PassArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Launch configuration per FFT length and precision.
+// Launch configuration per FFT length and precision (column passes above
+// N = 1024 FP32 / 512 FP64 use 256-thread CTAs so that a thread may hold 255
+// registers: the 32-value transforms spill badly at 128).
 template <typename Rl, int N> struct RowCfg;
 template <typename Rl, int N> struct ColCfg;
 // float: T threads per transform, RV = N / T values per thread
@@ -58,14 +60,14 @@ template <> struct ColCfg<float, 128> { static constexpr int T = 16, CP = 32, MI
 template <> struct ColCfg<float, 256> { static constexpr int T = 32, CP = 16, MINB = 1; };
 template <> struct ColCfg<float, 512> { static constexpr int T = 32, CP = 16, MINB = 1; };
 template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 8, MINB = 1; };
-template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 8, MINB = 1; };
-template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 4, MINB = 1; };
+template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 4, MINB = 1; };
+template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 2, MINB = 1; };
 template <> struct ColCfg<double, 128> { static constexpr int T = 16, CP = 16, MINB = 1; };
 template <> struct ColCfg<double, 256> { static constexpr int T = 16, CP = 16, MINB = 1; };
 template <> struct ColCfg<double, 512> { static constexpr int T = 32, CP = 8, MINB = 1; };
-template <> struct ColCfg<double, 1024> { static constexpr int T = 64, CP = 8, MINB = 1; };
-template <> struct ColCfg<double, 2048> { static constexpr int T = 128, CP = 4, MINB = 1; };
-template <> struct ColCfg<double, 4096> { static constexpr int T = 256, CP = 2, MINB = 1; };
+template <> struct ColCfg<double, 1024> { static constexpr int T = 64, CP = 4, MINB = 1; };
+template <> struct ColCfg<double, 2048> { static constexpr int T = 128, CP = 2, MINB = 1; };
+template <> struct ColCfg<double, 4096> { static constexpr int T = 256, CP = 1, MINB = 1; };
 
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
