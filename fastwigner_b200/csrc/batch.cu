@@ -63,7 +63,9 @@ template <int V> struct BRow<256, V> { static constexpr int T = 32, G = 8; };
 template <int V> struct BRow<512, V> { static constexpr int T = (V == 0 ? 32 : 64), G = BT / T; };
 template <int V> struct BRow<1024, V> { static constexpr int T = (V == 0 ? 32 : 64), G = BT / T; };
 
-template <int N, int V> constexpr size_t bcol_smem() { return (size_t)2 * N * BCol<N, V>::CP * sizeof(float); }
+template <int N, int V> constexpr size_t bcol_smem() {
+  return col_ex_reals<float, N, BCol<N, V>::T, BCol<N, V>::CP>() * sizeof(float);
+}
 template <int N, int V> constexpr size_t brow_smem() {
   return (size_t)BRow<N, V>::G * 2 * (N + N / 32) * sizeof(float);
 }
@@ -131,7 +133,7 @@ __device__ __forceinline__ void do_col(const BatchArgs& a, const BatchInst& in, 
 #define COLN(N_)                                                                                            \
   case N_: {                                                                                                \
     constexpr int T = BCol<N_, V>::T, CP = BCol<N_, V>::CP;                                                 \
-    col_tile<float, N_, T, CP, ilog2_c(N_ / T > 32 ? 32 : N_ / T)>(p, 0, tile, in.ncol, smem, red, ored);   \
+    col_tile<float, N_, T, CP>(p, 0, tile, in.ncol, smem, red, ored);                                        \
   } break;
     COLN(128) COLN(256) COLN(512) COLN(1024)
 #undef COLN

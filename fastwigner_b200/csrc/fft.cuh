@@ -93,6 +93,8 @@ template <int DIR, typename C> struct DFT<1, DIR, C> {
   static __device__ __forceinline__ void run(C*) {}
 };
 
+constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n / 2); }
+
 // Stockham radix-R stage chain.  EX is the exchange object (shared memory
 // layout + synchronisation scope of the group).  tw: table of exp(-2 pi i k/N),
 // k < N, readable by every thread (shared or global memory).
@@ -104,6 +106,12 @@ __device__ __forceinline__ void stockham(C (&v)[RV], const int j, EX& ex, const 
   constexpr int Q = RV / R;
   constexpr bool FIRST = (NS == 1);
   constexpr bool LAST = (NS * R == N);
+  // Address folding: with a layout padded once per 2^L elements (L = log2 RV)
+  // and T >= RV, every in-stage offset (q*T + r*N/R on reads, r*NS on writes)
+  // is a multiple of 2^L, or a write offset r < RV from an RV-aligned base, so
+  // map(base + d) = map(base) + delta(d) and the per-access address is one
+  // per-thread register plus an immediate.
+  constexpr bool FOLD = EX::kFold && EX::kL == ilog2_c(RV) && T >= RV;
   static_assert(R >= 2 && (RV % R) == 0, "bad radix plan");
   C u[RV];
   if constexpr (FIRST) {
@@ -112,10 +120,14 @@ __device__ __forceinline__ void stockham(C (&v)[RV], const int j, EX& ex, const 
 #pragma unroll
       for (int r = 0; r < R; ++r) u[q * R + r] = v[q + r * Q];
   } else {
+    const int aj = ex.map(j);  // per-thread part of every read address of this stage
 #pragma unroll
     for (int q = 0; q < Q; ++q)
 #pragma unroll
-      for (int r = 0; r < R; ++r) u[q * R + r] = ex.read(j + q * T + r * (N / R));
+      for (int r = 0; r < R; ++r) {
+        const int d = q * T + r * (N / R);
+        u[q * R + r] = ex.read_at(FOLD ? aj + ex.delta(d) : ex.map(j + d));
+      }
     ex.sync();
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -140,8 +152,9 @@ __device__ __forceinline__ void stockham(C (&v)[RV], const int j, EX& ex, const 
     for (int q = 0; q < Q; ++q) {
       const int b = j + q * T;
       const int base = (b / NS) * NS * R + (b & (NS - 1));
+      const int ab = ex.map(base);
 #pragma unroll
-      for (int r = 0; r < R; ++r) ex.write(base + r * NS, u[q * R + r]);
+      for (int r = 0; r < R; ++r) ex.write_at(FOLD ? ab + ex.delta(r * NS) : ex.map(base + r * NS), u[q * R + r]);
     }
     ex.sync();
     stockham<N, T, RV, NS * R, DIR, C, EX>(v, j, ex, tw);
@@ -153,7 +166,15 @@ __device__ __forceinline__ void fft(C (&v)[RV], const int j, EX& ex, const C* __
   stockham<N, T, RV, 1, DIR, C, EX>(v, j, ex, tw);
 }
 
-constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n / 2); }
+// Write v[m] (natural order: element j + m*T) into the exchange buffer,
+// folding the addresses when the layout allows it (see stockham).
+template <int T, int RV, typename EX, typename C>
+__device__ __forceinline__ void ex_write_natural(const EX& ex, const int j, const C (&v)[RV]) {
+  constexpr bool FOLD = EX::kFold && EX::kL == ilog2_c(RV) && T >= RV;
+  const int aj = ex.map(j);
+#pragma unroll
+  for (int m = 0; m < RV; ++m) ex.write_at(FOLD ? aj + ex.delta(m * T) : ex.map(j + m * T), v[m]);
+}
 
 // Named barrier over `nthreads` threads (multiple of 32) with id 1..15.
 __device__ __forceinline__ void named_barrier(int id, int nthreads) {
@@ -168,9 +189,15 @@ template <typename Rl, int T> struct GroupEx {
   Rl* im;
   int bar_id;  // used only when T > 32
   using C = cplx_t<Rl>;
+  static constexpr int kL = 5;
+  static constexpr bool kFold = true;
   __device__ __forceinline__ static int pad(int i) { return i + (i >> 5); }
-  __device__ __forceinline__ C read(int i) const { const int a = pad(i); return mk<C>(re[a], im[a]); }
-  __device__ __forceinline__ void write(int i, C v) const { const int a = pad(i); re[a] = v.x; im[a] = v.y; }
+  __device__ __forceinline__ static int map(int i) { return pad(i); }
+  __device__ __forceinline__ static constexpr int delta(int d) { return d + (d >> 5); }
+  __device__ __forceinline__ C read_at(int a) const { return mk<C>(re[a], im[a]); }
+  __device__ __forceinline__ void write_at(int a, C v) const { re[a] = v.x; im[a] = v.y; }
+  __device__ __forceinline__ C read(int i) const { return read_at(pad(i)); }
+  __device__ __forceinline__ void write(int i, C v) const { write_at(pad(i), v); }
   __device__ __forceinline__ void sync() const {
     if constexpr (T <= 32) __syncwarp();
     else named_barrier(bar_id, T);
@@ -187,9 +214,37 @@ template <typename Rl, int CP, int S> struct ColEx {
   Rl* im;
   int c;
   using C = cplx_t<Rl>;
-  __device__ __forceinline__ int addr(int i) const { return (i ^ ((i >> S) & 1)) * CP + c; }
-  __device__ __forceinline__ C read(int i) const { const int a = addr(i); return mk<C>(re[a], im[a]); }
-  __device__ __forceinline__ void write(int i, C v) const { const int a = addr(i); re[a] = v.x; im[a] = v.y; }
+  static constexpr int kL = 0;
+  static constexpr bool kFold = false;
+  __device__ __forceinline__ int map(int i) const { return (i ^ ((i >> S) & 1)) * CP + c; }
+  __device__ __forceinline__ static constexpr int delta(int) { return 0; }
+  __device__ __forceinline__ C read_at(int a) const { return mk<C>(re[a], im[a]); }
+  __device__ __forceinline__ void write_at(int a, C v) const { re[a] = v.x; im[a] = v.y; }
+  __device__ __forceinline__ C read(int i) const { return read_at(map(i)); }
+  __device__ __forceinline__ void write(int i, C v) const { write_at(map(i), v); }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// Exchange for the column passes with a padded instead of a swizzled layout:
+// element i of FFT c at slot (i + (i >> L)) * CP + c, one pad slot per 2^L
+// elements (L = log2 RV).  With 32/CP consecutive transform threads per warp
+// the Stockham reads and writes, and the natural-order mid-point accesses,
+// fall in distinct banks, and every in-stage address folds into a
+// per-thread base plus an immediate.  Each component array holds
+// (N + N/2^L) * CP reals.  Synchronisation is CTA-wide.
+template <typename Rl, int CP, int L> struct ColPadEx {
+  Rl* re;
+  Rl* im;
+  int c;
+  using C = cplx_t<Rl>;
+  static constexpr int kL = L;
+  static constexpr bool kFold = true;
+  __device__ __forceinline__ int map(int i) const { return (i + (i >> L)) * CP + c; }
+  __device__ __forceinline__ static constexpr int delta(int d) { return (d + (d >> L)) * CP; }
+  __device__ __forceinline__ C read_at(int a) const { return mk<C>(re[a], im[a]); }
+  __device__ __forceinline__ void write_at(int a, C v) const { re[a] = v.x; im[a] = v.y; }
+  __device__ __forceinline__ C read(int i) const { return read_at(map(i)); }
+  __device__ __forceinline__ void write(int i, C v) const { write_at(map(i), v); }
   __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 

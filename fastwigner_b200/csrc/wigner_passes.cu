@@ -15,12 +15,12 @@ __global__ void __launch_bounds__(G* T, MINB) row_pass_kernel(PassArgs a) {
   row_tile<Rl, N, T, G>(a, blockIdx.y, blockIdx.x, smem_raw, red);
 }
 
-template <typename Rl, int N, int T, int CP, int S, int MINB>
+template <typename Rl, int N, int T, int CP, int MINB>
 __global__ void __launch_bounds__(CP* T, MINB) col_pass_kernel(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[34];
   __shared__ double ored[(CP * T) / 32][2 + 2 * MAXO];
-  col_tile<Rl, N, T, CP, S>(a, blockIdx.y, blockIdx.x, gridDim.x, smem_raw, red, ored);
+  col_tile<Rl, N, T, CP>(a, blockIdx.y, blockIdx.x, gridDim.x, smem_raw, red, ored);
 }
 
 // ---------------------------------------------------------------------------
@@ -92,9 +92,8 @@ template <typename Rl, int N>
 static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts) {
   using Cfg = ColCfg<Rl, N>;
   constexpr int T = Cfg::T, CP = Cfg::CP, MINB = Cfg::MINB;
-  constexpr int S = ilog2(N / T > 32 ? 32 : N / T);
-  const size_t smem = (size_t)2 * N * CP * sizeof(Rl);
-  auto kern = col_pass_kernel<Rl, N, T, CP, S, MINB>;
+  const size_t smem = col_ex_reals<Rl, N, T, CP>() * sizeof(Rl);
+  auto kern = col_pass_kernel<Rl, N, T, CP, MINB>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

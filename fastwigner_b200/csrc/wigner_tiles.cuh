@@ -35,8 +35,7 @@ __device__ __forceinline__ void spectral_mul(cplx_t<Rl> (&v)[RV], const int j, E
                                              const void* tabb, size_t tab_stride, int tab_real, const void* g,
                                              Rl f) {
   using C = cplx_t<Rl>;
-#pragma unroll
-  for (int m = 0; m < RV; ++m) ex.write(j + m * T, v[m]);
+  ex_write_natural<T, RV>(ex, j, v);
   ex.sync();
 #pragma unroll
   for (int m = 0; m < RV; ++m) {
@@ -167,8 +166,7 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
   const C* G = reinterpret_cast<const C*>(a.wph) + (size_t)b * a.wph_bs;
   const bool obs = a.part_out != nullptr;
   const Rl h = (Rl)(0.5 / (double)N);
-#pragma unroll
-  for (int m = 0; m < RV; ++m) ex.write(j + m * T, v[m]);
+  ex_write_natural<T, RV>(ex, j, v);
   ex.sync();
   o.s2 = 0;
   o.ca = 0;
@@ -265,7 +263,11 @@ __device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, in
 
 // One work item of a column pass: instance b, column pairs tile*CP .. tile*CP+CP-1
 // (ntiles = X / (2 CP) tiles per instance, the partial-sum records per instance).
-template <typename Rl, int N, int T, int CP, int S>
+// Reals of shared memory a column tile's exchange buffer takes: CP
+// interleaved transforms, two components, one pad slot per RV = N/T elements.
+template <typename Rl, int N, int T, int CP> constexpr size_t col_ex_reals() { return (size_t)2 * (N + T) * CP; }
+
+template <typename Rl, int N, int T, int CP>
 __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int ntiles, unsigned char* smem_raw,
                                          double* red, double (*ored)[2 + 2 * MAXO]) {
   using C = cplx_t<Rl>;
@@ -277,7 +279,7 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
   const int X = a.X;
   const int xa = tile * 2 * CP + 2 * c;
   Rl* re = reinterpret_cast<Rl*>(smem_raw);
-  ColEx<Rl, CP, S> ex{re, re + (size_t)N * CP, c};
+  ColPadEx<Rl, CP, ilog2_c(RV)> ex{re, re + (size_t)(N + T) * CP, c};
   Rl* W = reinterpret_cast<Rl*>(a.W) + (size_t)b * a.w_bs;
   const C* tw = reinterpret_cast<const C*>(a.tw);
   C v[RV];
