@@ -11,6 +11,7 @@ One bench step = one time step of every instance of the batch (two fused
 passes per instance).  value = grid-point steps per second over all ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --workload {moyal_fp64_256,vn_1024,bloch_512,batch_uneven,strong_field}
 
 Under torchrun (N > 1) every rank advances its own batch (different seeds,
 no data-path collective): weak scaling, time = max over ranks.
@@ -343,11 +344,20 @@ def main():
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="moyal_1024",
+                    help="moyal_1024 (the default line) or one of fastwigner_b200.benchmarks.WORKLOADS")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "moyal_1024":
+        from fastwigner_b200 import benchmarks
+
+        if args.workload not in benchmarks.WORKLOADS:
+            ap.error(f"unknown workload {args.workload}")
+        print(json.dumps(benchmarks.run(args.workload)), flush=True)
+        return 0
     return run_ours(args)
 
 

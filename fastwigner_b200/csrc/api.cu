@@ -28,8 +28,27 @@ static std::vector<double> twiddles(int n) {
   return t;
 }
 
-static int upload_twiddles(int n, int dtype, void** dev) {
-  std::vector<double> t = twiddles(n);
+// Stage-layout twiddle table of an n-point transform with rv values per
+// thread (fft.cuh, stage_off): the entries of twiddles(n) at k = bm r n/(ns R),
+// computed by the same expression, so both tables hold identical values.
+static std::vector<double> stage_twiddles(int n, int rv) {
+  std::vector<double> t;
+  for (int ns = rv; ns < n; ns *= rv) {
+    const int R = n / ns >= rv ? rv : n / ns;
+    const int s = n / (ns * R);
+    for (int r = 1; r < R; ++r)
+      for (int bm = 0; bm < ns; ++bm) {
+        const double a = -2.0 * M_PI * (double)(bm * r * s) / (double)n;
+        t.push_back(cos(a));
+        t.push_back(sin(a));
+      }
+  }
+  if (t.empty()) t.assign(2, 0.0);
+  return t;
+}
+
+static int upload_twiddles(int n, int dtype, void** dev, int rv = 0) {
+  std::vector<double> t = rv > 0 ? stage_twiddles(n, rv) : twiddles(n);
   cudaError_t e;
   if (dtype == FW_F64) {
     e = cudaMalloc(dev, t.size() * sizeof(double));
@@ -54,11 +73,13 @@ struct fw_wigner_plan {
   int nparts;          // column-pass CTAs per instance (partials per instance)
   void* twP = nullptr; // twiddles for length P
   void* twX = nullptr; // twiddles for length X
+  void* twsX = nullptr; // stage-layout twiddles of the row pass (length X)
   double* ring = nullptr;  // 2 x batch x nparts x MMAX partial sums
   double* wsum = nullptr;  // scratch for fw_wigner_weighted_sum partials
   int wsum_blocks = 0;
   void* wph = nullptr;  // spectra of the p-observable weights (wph_nb x 4 x P complex)
   int wph_nb = 0;
+  double* tot = nullptr;  // per-instance reduced partial sums (batch x MMAX)
 };
 
 static constexpr int MMAX = 2 + 8;
@@ -81,6 +102,7 @@ extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wign
   p->P = P; p->X = X; p->batch = batch; p->dtype = dtype; p->nparts = np;
   int rc = upload_twiddles(P, dtype, &p->twP);
   if (rc == FW_OK) rc = upload_twiddles(X, dtype, &p->twX);
+  if (rc == FW_OK) rc = upload_twiddles(X, dtype, &p->twsX, row_rv(dtype, X));
   if (rc == FW_OK) {
     cudaError_t e = cudaMalloc(&p->ring, sizeof(double) * 2 * (size_t)batch * np * MMAX);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(partials)");
@@ -97,6 +119,10 @@ extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wign
     cudaError_t e = cudaMalloc(&p->wph, per * p->wph_nb);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(weight spectra)");
   }
+  if (rc == FW_OK) {
+    cudaError_t e = cudaMalloc(&p->tot, sizeof(double) * (size_t)batch * MMAX);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(instance totals)");
+  }
   if (rc != FW_OK) {
     fw_wigner_plan_destroy(p);
     return rc;
@@ -109,9 +135,11 @@ extern "C" int fw_wigner_plan_destroy(fw_wigner_plan* p) {
   if (p == nullptr) return FW_OK;
   cudaFree(p->twP);
   cudaFree(p->twX);
+  cudaFree(p->twsX);
   cudaFree(p->ring);
   cudaFree(p->wsum);
   cudaFree(p->wph);
+  cudaFree(p->tot);
   delete p;
   return FW_OK;
 }
@@ -188,6 +216,11 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   auto ring = [&](int k) { return plan->ring + (size_t)(k & 1) * ring_slot; };
   auto hist = [&](int k) { return d->obs_out == nullptr ? nullptr : d->obs_out + (size_t)k * B * M; };
 
+  // With a totals buffer, a small kernel after each column pass with partial
+  // sums reduces them per instance (and records the observable history); the
+  // next pass reads one total per instance.  Without it (fixed-scratch plans)
+  // every CTA of the next pass reduces the partials itself.
+  const bool totals = plan->tot != nullptr;
   auto col = [&](PassArgs a) -> int {
     a.tw = plan->twP;
     int np = 0;
@@ -195,10 +228,16 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
     if (e != cudaSuccess) return cuda_fail(e, "column pass launch");
     ++g_launches;
     if (g_timer) g_timer->mark(0);
+    if (totals && a.part_out != nullptr) {
+      e = launch_totals(a.part_out, plan->nparts, M, B, plan->tot, a.obs_hist, st);
+      if (e != cudaSuccess) return cuda_fail(e, "totals launch");
+      ++g_launches;
+      if (g_timer) g_timer->mark(3);
+    }
     return FW_OK;
   };
   auto row = [&](PassArgs a) -> int {
-    a.tw = plan->twX;
+    a.tw = plan->twsX;
     cudaError_t e = launch_row(a, plan->dtype, st);
     if (e != cudaSuccess) return cuda_fail(e, "row pass launch");
     ++g_launches;
@@ -209,8 +248,13 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
     a.part_out = ring(k);
     a.wx = d->wx == nullptr ? nullptr : d->wx + (size_t)k * d->wx_step;
     a.wp = d->wp == nullptr ? nullptr : d->wp + (size_t)k * d->wp_step;
+    if (totals) a.obs_hist = hist(k);  // read by the totals kernel, not by the pass
   };
   auto prev_args = [&](PassArgs& a, int k) {  // normalisation from the partials of step k
+    if (totals) {
+      a.prev_tot = plan->tot;
+      return;
+    }
     a.prev_part = ring(k);
     a.prev_nparts = plan->nparts;
     a.obs_hist = hist(k);
@@ -399,6 +443,25 @@ __global__ void noalloc_twiddles_kernel(int n, int dtype, void* out) {
   }
 }
 
+// Stage-layout table (fft.cuh, stage_off) of an n-point transform with rv
+// values per thread, gathered from the k-indexed table tw; total entries.
+__global__ void noalloc_stage_kernel(int n, int rv, int dtype, const void* tw, void* out, int total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int ns = rv, off = 0, R = rv;
+  for (;;) {  // i < total bounds the walk over the stages
+    R = n / ns >= rv ? rv : n / ns;
+    const int sz = (R - 1) * ns;
+    if (i < off + sz) break;
+    off += sz;
+    ns *= rv;
+  }
+  const int r = (i - off) / ns + 1, bm = (i - off) % ns;
+  const int k = bm * r * (n / (ns * R));
+  if (dtype == FW_F64) reinterpret_cast<double2*>(out)[i] = reinterpret_cast<const double2*>(tw)[k];
+  else reinterpret_cast<float2*>(out)[i] = reinterpret_cast<const float2*>(tw)[k];
+}
+
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 }  // namespace
 
@@ -416,8 +479,11 @@ extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, c
   const size_t rs = dtype == FW_F64 ? sizeof(double) : sizeof(float);
   const size_t twP_bytes = align256(2 * rs * (size_t)P);
   const size_t twX_bytes = align256(2 * rs * (size_t)X);
+  const int rvX = row_rv(dtype, X);
+  const int nsX = stage_off(X, rvX, X);
+  const size_t twsX_bytes = align256(2 * rs * (size_t)(nsX > 0 ? nsX : 1));
   const size_t ring_bytes = sizeof(double) * 2 * (size_t)batch * np * MMAX;
-  const size_t need = twP_bytes + twX_bytes + ring_bytes;
+  const size_t need = twP_bytes + twX_bytes + twsX_bytes + ring_bytes;
   if (need > kNoAllocScratchBytes)
     return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: needs " + std::to_string(need) +
                                " bytes of scratch for this grid and batch, more than the fixed " +
@@ -438,9 +504,11 @@ extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, c
   // the partial-sum ring is always written before it is read
   noalloc_twiddles_kernel<<<(P + 255) / 256, 256, 0, st>>>(P, dtype, base);
   noalloc_twiddles_kernel<<<(X + 255) / 256, 256, 0, st>>>(X, dtype, base + twP_bytes);
+  unsigned char* twsX = base + twP_bytes + twX_bytes;
+  if (nsX > 0) noalloc_stage_kernel<<<(nsX + 255) / 256, 256, 0, st>>>(X, rvX, dtype, base + twP_bytes, twsX, nsX);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "noalloc twiddle launch");
-  count_launch(2);
+  count_launch(2 + (nsX > 0));
   fw_wigner_plan tmp;
   tmp.P = P;
   tmp.X = X;
@@ -449,7 +517,8 @@ extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, c
   tmp.nparts = np;
   tmp.twP = base;
   tmp.twX = base + twP_bytes;
-  tmp.ring = reinterpret_cast<double*>(base + twP_bytes + twX_bytes);
+  tmp.twsX = twsX;
+  tmp.ring = reinterpret_cast<double*>(twsX + twsX_bytes);
   tmp.wsum = nullptr;
   tmp.wsum_blocks = 0;
   return fw_wigner_propagate(&tmp, desc, steps, stream);

@@ -95,10 +95,21 @@ template <int DIR, typename C> struct DFT<1, DIR, C> {
 
 constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n / 2); }
 
+// Stage-layout twiddle table of an N-point transform with RV values per
+// thread: for every stage with stride NS > 1 (radix R = min(RV, N/NS)) the
+// entries w^(bm r N/(NS R)), r = 1..R-1, bm = 0..NS-1, stored [r-1][bm] so a
+// warp's consecutive bm read consecutive entries.  stage_off(NS) is the
+// offset of that stage; stage_off(N) the table length.
+__host__ __device__ constexpr int stage_off(int N, int RV, int NS) {
+  int off = 0;
+  for (int ns = RV; ns < NS; ns *= RV) off += ((N / ns >= RV ? RV : N / ns) - 1) * ns;
+  return off;
+}
+
 // Stockham radix-R stage chain.  EX is the exchange object (shared memory
 // layout + synchronisation scope of the group).  tw: table of exp(-2 pi i k/N),
 // k < N, readable by every thread (shared or global memory).
-template <int N, int T, int RV, int NS, int DIR, typename C, typename EX>
+template <int N, int T, int RV, int NS, int DIR, typename C, typename EX, bool STW = false>
 __device__ __forceinline__ void stockham(C (&v)[RV], const int j, EX& ex, const C* __restrict__ tw) {
   static_assert(N == RV * T, "N must equal RV*T");
   constexpr int REM = N / NS;
@@ -134,7 +145,7 @@ __device__ __forceinline__ void stockham(C (&v)[RV], const int j, EX& ex, const 
       const int bm = (j + q * T) & (NS - 1);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        C w = tw[bm * r * (N / (NS * R))];
+        C w = STW ? tw[stage_off(N, RV, NS) + (r - 1) * NS + bm] : tw[bm * r * (N / (NS * R))];
         if (DIR > 0) w = cconj(w);
         u[q * R + r] = cmul(u[q * R + r], w);
       }
@@ -157,13 +168,15 @@ __device__ __forceinline__ void stockham(C (&v)[RV], const int j, EX& ex, const 
       for (int r = 0; r < R; ++r) ex.write_at(FOLD ? ab + ex.delta(r * NS) : ex.map(base + r * NS), u[q * R + r]);
     }
     ex.sync();
-    stockham<N, T, RV, NS * R, DIR, C, EX>(v, j, ex, tw);
+    stockham<N, T, RV, NS * R, DIR, C, EX, STW>(v, j, ex, tw);
   }
 }
 
-template <int N, int T, int RV, int DIR, typename C, typename EX>
+// tw: the table exp(-2 pi i k/N), k < N (STW = false) or the stage-layout
+// table of (N, RV) (STW = true).
+template <int N, int T, int RV, int DIR, typename C, typename EX, bool STW = false>
 __device__ __forceinline__ void fft(C (&v)[RV], const int j, EX& ex, const C* __restrict__ tw) {
-  stockham<N, T, RV, 1, DIR, C, EX>(v, j, ex, tw);
+  stockham<N, T, RV, 1, DIR, C, EX, STW>(v, j, ex, tw);
 }
 
 // Write v[m] (natural order: element j + m*T) into the exchange buffer,

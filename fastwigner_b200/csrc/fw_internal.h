@@ -11,7 +11,10 @@ cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* npart
 cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st);
 cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P, int nb, void* out, long long out_bs,
                                int dtype, cudaStream_t st);
+cudaError_t launch_totals(const double* part, int nparts, int M, int batch, double* tot, double* hist,
+                          cudaStream_t st);
 int col_parts(int dtype, int P, int X);
+int row_rv(int dtype, int N);
 bool size_supported(int n);
 
 void set_error(const std::string& msg);

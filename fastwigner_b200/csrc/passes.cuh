@@ -65,11 +65,16 @@ struct PassArgs {
   int fuse_mid;
   const void* wph;  // complex, same precision as W
   long long wph_bs;
+  // Per-instance totals of the previous pass's partial sums (reduced by
+  // totals_kernel, M doubles per instance): the input scale is read from
+  // prev_tot[b*M] instead of reducing prev_part in every CTA.
+  const double* prev_tot;
 };
 
 // Reduce previous-pass partial sums (per instance) into the input scale.
 // Called by every thread; uses `red` (>= 33 doubles of shared memory).
 __device__ __forceinline__ double prev_scale(const PassArgs& a, int b, double* red, bool first_tile) {
+  if (a.prev_tot != nullptr) return 1.0 / (__ldcg(a.prev_tot + (size_t)b * a.M) * a.dxdp);
   if (a.prev_part == nullptr) return a.scale_const;
   const int tid = threadIdx.x;
   const int nth = blockDim.x;

@@ -12,7 +12,7 @@ template <typename Rl, int N, int T, int G, int MINB>
 __global__ void __launch_bounds__(G* T, MINB) row_pass_kernel(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[34];
-  row_tile<Rl, N, T, G>(a, blockIdx.y, blockIdx.x, smem_raw, red);
+  row_tile<Rl, N, T, G, true>(a, blockIdx.y, blockIdx.x, smem_raw, red);
 }
 
 template <typename Rl, int N, int T, int CP, int MINB>
@@ -21,6 +21,25 @@ __global__ void __launch_bounds__(CP* T, MINB) col_pass_kernel(PassArgs a) {
   __shared__ double red[34];
   __shared__ double ored[(CP * T) / 32][2 + 2 * MAXO];
   col_tile<Rl, N, T, CP>(a, blockIdx.y, blockIdx.x, gridDim.x, smem_raw, red, ored);
+}
+
+// Per-instance totals of a pass's partial-sum records: block b, thread m < M
+// sums column m of instance b's records in record order (deterministic) into
+// tot[b*M + m], and into hist[b*M + m] when hist is set.
+__global__ void totals_kernel(const double* part, int nparts, int M, double* tot, double* hist) {
+  const int b = blockIdx.x, m = threadIdx.x;
+  if (m >= M) return;
+  const double* pp = part + (size_t)b * nparts * M + m;
+  double s = 0.0;
+  for (int c = 0; c < nparts; ++c) s += pp[(size_t)c * M];
+  tot[(size_t)b * M + m] = s;
+  if (hist != nullptr) hist[(size_t)b * M + m] = s;
+}
+
+cudaError_t launch_totals(const double* part, int nparts, int M, int batch, double* tot, double* hist,
+                          cudaStream_t st) {
+  totals_kernel<<<batch, 32, 0, st>>>(part, nparts, M, tot, hist);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -116,6 +135,16 @@ int col_parts(int dtype, int P, int X) {
   return X / (2 * cp);
 }
 
+// Values per thread of the row pass transform of length N (the radix plan
+// its stage-layout twiddle table is built for).
+int row_rv(int dtype, int N) {
+  int t = 0;
+#define RT(R, N_) if (N == N_) t = RowCfg<R, N_>::T;
+  if (dtype == FW_F32) { RT(float, 128) RT(float, 256) RT(float, 512) RT(float, 1024) RT(float, 2048) RT(float, 4096) }
+  else { RT(double, 128) RT(double, 256) RT(double, 512) RT(double, 1024) RT(double, 2048) RT(double, 4096) }
+#undef RT
+  return t > 0 ? N / t : 0;
+}
 bool size_supported(int n) { return n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096; }
 
 cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st) {

@@ -51,7 +51,8 @@ __device__ __forceinline__ void spectral_mul(cplx_t<Rl> (&v)[RV], const int j, E
 // ---------------------------------------------------------------------------
 // Row pass: G groups of T threads, each group owns one pair of rows.
 // One CTA-sized work item of a row pass: instance b, row pairs blk*G .. blk*G+G-1.
-template <typename Rl, int N, int T, int G>
+// STW: a.tw is the stage-layout twiddle table of (N, N/T) instead of exp(-2 pi i k/N).
+template <typename Rl, int N, int T, int G, bool STW = false>
 __device__ __forceinline__ void row_tile(const PassArgs& a, int b, int blk, unsigned char* smem_raw, double* red) {
   using C = cplx_t<Rl>;
   constexpr int RV = N / T;
@@ -63,6 +64,7 @@ __device__ __forceinline__ void row_tile(const PassArgs& a, int b, int blk, unsi
   constexpr int BUF = N + N / 32;
   Rl* base = reinterpret_cast<Rl*>(smem_raw) + (size_t)g * 2 * BUF;
   GroupEx<Rl, T> ex{base, base + BUF, 1 + g};
+  using EXT = GroupEx<Rl, T>;
   Rl* W = reinterpret_cast<Rl*>(a.W) + (size_t)b * a.w_bs + (size_t)(2 * rp) * N;
   const C* tw = reinterpret_cast<const C*>(a.tw);
   C v[RV];
@@ -72,13 +74,13 @@ __device__ __forceinline__ void row_tile(const PassArgs& a, int b, int blk, unsi
     const int x = j + m * T;
     v[m] = mk<C>(__ldcg(W + x) * s, __ldcg(W + N + x) * s);
   }
-  fft<N, T, RV, -1>(v, j, ex, tw);
+  fft<N, T, RV, -1, C, EXT, STW>(v, j, ex, tw);
   const size_t esz = a.tab_real ? sizeof(Rl) : sizeof(C);
   const size_t hs = N / 2 + 1;
   const char* tb = reinterpret_cast<const char*>(a.tab1) + ((size_t)b * a.tab_bs + (size_t)(2 * rp) * hs) * esz;
   const Rl f = (Rl)(a.out_scale / (double)N);
   spectral_mul<Rl, N, T, RV>(v, j, ex, tb, tb + hs * esz, 1, a.tab_real, a.g1, f);
-  fft<N, T, RV, +1>(v, j, ex, tw);
+  fft<N, T, RV, +1, C, EXT, STW>(v, j, ex, tw);
 #pragma unroll
   for (int m = 0; m < RV; ++m) {
     const int x = j + m * T;
@@ -267,7 +269,7 @@ __device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, in
 // interleaved transforms, two components, one pad slot per RV = N/T elements.
 template <typename Rl, int N, int T, int CP> constexpr size_t col_ex_reals() { return (size_t)2 * (N + T) * CP; }
 
-template <typename Rl, int N, int T, int CP>
+template <typename Rl, int N, int T, int CP, bool STW = false>
 __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int ntiles, unsigned char* smem_raw,
                                          double* red, double (*ored)[2 + 2 * MAXO]) {
   using C = cplx_t<Rl>;
@@ -279,7 +281,8 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
   const int X = a.X;
   const int xa = tile * 2 * CP + 2 * c;
   Rl* re = reinterpret_cast<Rl*>(smem_raw);
-  ColPadEx<Rl, CP, ilog2_c(RV)> ex{re, re + (size_t)(N + T) * CP, c};
+  using EXT = ColPadEx<Rl, CP, ilog2_c(RV)>;
+  EXT ex{re, re + (size_t)(N + T) * CP, c};
   Rl* W = reinterpret_cast<Rl*>(a.W) + (size_t)b * a.w_bs;
   const C* tw = reinterpret_cast<const C*>(a.tw);
   C v[RV];
@@ -301,21 +304,21 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
     }
   }
   if (a.fuse_mid) {
-    fft<N, T, RV, -1>(v, j, ex, tw);
+    fft<N, T, RV, -1, C, EXT, STW>(v, j, ex, tw);
     MidSums<Rl> o;
     fused_mid<Rl, N, T, RV>(a, b, v, j, ex, xa, o);
     if (a.part_out != nullptr) mid_store<Rl, N, CP, CP * T>(a, b, tile, ntiles, o, xa, ored);
-    fft<N, T, RV, +1>(v, j, ex, tw);
+    fft<N, T, RV, +1, C, EXT, STW>(v, j, ex, tw);
     col_store<Rl, N, T, RV>(a, v, W, j, xa);
     return;
   }
   const size_t esz = a.tab_real ? sizeof(Rl) : sizeof(C);
   const Rl f = (Rl)(1.0 / (double)N);
   if (a.tab1 != nullptr) {
-    fft<N, T, RV, -1>(v, j, ex, tw);
+    fft<N, T, RV, -1, C, EXT, STW>(v, j, ex, tw);
     const char* tb = reinterpret_cast<const char*>(a.tab1) + ((size_t)b * a.tab_bs + xa) * esz;
     spectral_mul<Rl, N, T, RV>(v, j, ex, tb, tb + esz, (size_t)X, a.tab_real, a.g1, f);
-    fft<N, T, RV, +1>(v, j, ex, tw);
+    fft<N, T, RV, +1, C, EXT, STW>(v, j, ex, tw);
   }
   if (a.bxp != nullptr) {
     const Rl* B = reinterpret_cast<const Rl*>(a.bxp) + (size_t)b * a.bxp_bs;
@@ -402,10 +405,10 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
     obs_store<CP * T>(a, b, tile, ntiles, acc, ored);
   }
   if (a.tab2 != nullptr) {
-    fft<N, T, RV, -1>(v, j, ex, tw);
+    fft<N, T, RV, -1, C, EXT, STW>(v, j, ex, tw);
     const char* tb = reinterpret_cast<const char*>(a.tab2) + ((size_t)b * a.tab_bs + xa) * esz;
     spectral_mul<Rl, N, T, RV>(v, j, ex, tb, tb + esz, (size_t)X, a.tab_real, a.g2, f);
-    fft<N, T, RV, +1>(v, j, ex, tw);
+    fft<N, T, RV, +1, C, EXT, STW>(v, j, ex, tw);
   }
   col_store<Rl, N, T, RV>(a, v, W, j, xa);
 }

@@ -401,21 +401,45 @@ def normalise_params(P):
 class BlochSurrogate:
     """FNO + the thermal workload: training on plain-Bloch data and seeding."""
 
-    def __init__(self, setup: MorseBlochSetup, net: FNO2d | None = None, train_grid=128):
+    def __init__(self, setup: MorseBlochSetup, net: FNO2d | None = None, train_grid=128, residual=True):
         self.s, self.g = setup, int(train_grid)
         self.net = net or FNO2d(n_params=3, width=32, modes=(16, 16), layers=4, proj=128)
         self.xs = (setup.X / setup.XA).astype(np.float32)
         self.ps = (setup.P / setup.PA).astype(np.float32)
         st = setup.G // self.g
         self.xs_t, self.ps_t = self.xs[::st], self.ps[::st]
+        self.residual = bool(residual)
+        self._xp_full = (torch.tensor(setup.X), torch.tensor(setup.P))
+        self._xp_train = (torch.tensor(setup.X[::st]), torch.tensor(setup.P[::st]))
+
+    def baseline(self, P, full=True):
+        """Harmonic-approximation Gibbs state of each Morse well (rows of P:
+        D, a, beta), the thermal Wigner function of H_h = p^2/2 + w^2 (x-x_e)^2/2
+        with w = a sqrt(2 D): exp(-(2/w) tanh(beta w/2) H_h) (hbar = 1), each
+        normalised to unit sum on the full or the training grid; (n, g, g) FP32.
+        With `residual` the network learns the anharmonic correction to it."""
+        P = np.asarray(P, dtype=np.float64)
+        x, p = self._xp_full if full else self._xp_train
+        x, p = x.to(self.net.device), p.to(self.net.device)
+        w = torch.tensor(P[:, 1] * np.sqrt(2.0 * P[:, 0]), device=x.device)
+        c = (2.0 / w) * torch.tanh(0.5 * torch.tensor(P[:, 2], device=x.device) * w)
+        Hh = 0.5 * p[None, :, None] ** 2 + 0.5 * (w[:, None, None] * (x[None, None, :] - self.s.x_e)) ** 2
+        B = torch.exp(-c[:, None, None] * (Hh - Hh.amin(dim=(1, 2), keepdim=True)))
+        return (B / B.sum(dim=(1, 2), keepdim=True)).float()
 
     def train(self, P, S, epochs=20, batch=16, lr=2e-3, rng=None, log=None):
         """P: (N, 3) raw (D, a, beta); S: (N, g, g) states (normalised to unit sum)."""
         rng = rng or np.random.default_rng(0)
         X = normalise_params(P)
         N = len(X)
-        scale = S.abs().amax(dim=(1, 2), keepdim=True)  # per-sample scale: learn the shape
-        T = (S / scale).contiguous()
+        if not self.residual:
+            scale = S.abs().amax(dim=(1, 2), keepdim=True)  # per-sample scale: learn the shape
+            T = (S / scale).contiguous()
+        else:  # the correction to the harmonic baseline, in units of the baseline's peak
+            T = torch.empty_like(S)
+            for c0 in range(0, N, 512):
+                B = self.baseline(P[c0:c0 + 512], full=False)
+                T[c0:c0 + 512] = (S[c0:c0 + 512] - B) / B.amax(dim=(1, 2), keepdim=True)
         steps = epochs * (N // batch)
         losses = []
         it = 0
@@ -442,6 +466,10 @@ class BlochSurrogate:
             X = normalise_params(np.stack([Ds[c0:c0 + chunk], As[c0:c0 + chunk],
                                            np.full(len(Ds[c0:c0 + chunk]), beta)], axis=1))
             out = self.net.forward(X, self.xs, self.ps, cache=False)
+            if self.residual:
+                n = len(Ds[c0:c0 + chunk])
+                B = self.baseline(np.stack([Ds[c0:c0 + chunk], As[c0:c0 + chunk], np.full(n, beta)], axis=1))
+                out = B + B.amax(dim=(1, 2), keepdim=True) * out
             outs.append(out / (out.double().sum(dim=(1, 2), keepdim=True) * self.s.dX * self.s.dP).float())
         return torch.cat(outs)
 

@@ -33,7 +33,8 @@ def timed(fn):
 
 
 def run_study(runs=200, nbeta=100, epochs=12, batch=16, grid=512, train_grid=128, eval_betas=(5.0, 10.0, 20.0),
-              n_eval=16, refine_fraction=0.2, seed=0, width=32, modes=(16, 16), layers=4, log=print):
+              n_eval=16, refine_fraction=0.2, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
+              residual=True, log=print):
     rng = np.random.default_rng(seed)
     setup = MorseBlochSetup(grid=grid)
     betas = np.exp(np.linspace(np.log(0.1), np.log(20.0), nbeta))
@@ -41,9 +42,9 @@ def run_study(runs=200, nbeta=100, epochs=12, batch=16, grid=512, train_grid=128
     P, S = generate_dataset(setup, runs, betas, rng, train_grid=train_grid)
     t_data = time.time() - t0
     net = FNO2d(n_params=3, width=width, modes=modes, layers=layers, proj=128, seed=seed)
-    sur = BlochSurrogate(setup, net, train_grid=train_grid)
+    sur = BlochSurrogate(setup, net, train_grid=train_grid, residual=residual)
     t0 = time.time()
-    losses = sur.train(P, S, epochs=epochs, batch=batch, rng=rng,
+    losses = sur.train(P, S, epochs=epochs, batch=batch, lr=lr, rng=rng,
                        log=(lambda ep, l: log(f"epoch {ep}: loss {l:.3e}")) if log else None)
     torch.cuda.synchronize()
     t_train = time.time() - t0
@@ -69,7 +70,8 @@ def run_study(runs=200, nbeta=100, epochs=12, batch=16, grid=512, train_grid=128
         if log:
             log(json.dumps(results[-1]))
     return dict(data_seconds=t_data, train_seconds=t_train, final_loss=float(np.mean(losses[-50:])),
-                samples=int(len(P)), epochs=epochs, results=results)
+                samples=int(len(P)), epochs=epochs, residual=residual, train_grid=train_grid, width=width,
+                refine_fraction=refine_fraction, results=results)
 
 
 def main():
@@ -78,9 +80,17 @@ def main():
     ap.add_argument("--nbeta", type=int, default=100)
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--refine", type=float, default=0.2)
+    ap.add_argument("--train-grid", type=int, default=128)
+    ap.add_argument("--width", type=int, default=32)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--plain-target", action="store_true",
+                    help="learn the thermal state itself instead of the correction to the harmonic baseline")
+    ap.add_argument("--eval-betas", default="5,10,20")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
-    r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine)
+    r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine, train_grid=a.train_grid,
+                  width=a.width, lr=a.lr, residual=not a.plain_target,
+                  eval_betas=tuple(float(b) for b in a.eval_betas.split(",")))
     print(json.dumps(r))
     if a.out:
         with open(a.out, "w") as f:
