@@ -1,6 +1,7 @@
 // C ABI of libfastwigner: plan objects, step sequencing, error reporting.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <string>
 #include <vector>
@@ -300,6 +301,10 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
         c.tab2 = tabV(k + 1);
         c.g2 = gV(k + 1);
         c.fuse_mid = fuse ? 1 : 0;
+        // a column pair's two table entries load as one vector when both
+        // tables start on 16 bytes and the instance stride keeps pairs aligned
+        auto a16 = [](const void* t) { return (reinterpret_cast<uintptr_t>(t) & 15) == 0; };
+        c.tab_vec = (d->tab_bstride % 2 == 0 && a16(c.tab1) && a16(c.tab2)) ? 1 : 0;
       }
       if ((rc = col(c)) != FW_OK) return rc;
     }

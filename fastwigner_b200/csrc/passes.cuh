@@ -24,7 +24,8 @@ namespace fw {
 // share one transform pair, W = irfft( rfft(W) * tab1*g1 * tab2*g2 ), and the
 // partial sums come from the mid-point spectrum (Parseval): sum = DC bin,
 // sum W^2 = |spectrum|^2 / N, sum W wp = Re(spectrum . conj(wph)) / N with
-// wph[q] the forward DFT of wp[q] (wph_bs complex entries between instances).
+// wph[k][q] the forward DFT of wp[q] at bin k (wph_bs complex entries between
+// instances).
 //
 // scale_in = scale_const if prev_part == null, else 1/(sum_c prev_part[b][c][0] * dxdp).
 // When obs_hist != null, block 0 of every instance also writes the reduced
@@ -63,8 +64,9 @@ struct PassArgs {
   double out_scale;
   int* status;  // device status word (error flags); may be null
   int fuse_mid;
-  const void* wph;  // complex, same precision as W
+  const void* wph;  // complex, same precision as W, [b][k][4] (bin-major, 4 weights per bin)
   long long wph_bs;
+  int tab_vec;      // tab1/tab2 start on 16 bytes: a column pair's two entries load as one vector
   // Per-instance totals of the previous pass's partial sums (reduced by
   // totals_kernel, M doubles per instance): the input scale is read from
   // prev_tot[b*M] instead of reducing prev_part in every CTA.

@@ -182,7 +182,8 @@ cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st) {
 // Forward DFT Wh[k] = sum_p w[p] exp(-2 pi i k p / P) of each p-observable
 // weight vector, in FP64 (radix-2 Stockham through shared memory, one CTA per
 // vector, twiddles from sincospi of an exact power-of-two ratio), rounded once
-// to the state precision.  Block (q, b): vector q of instance b.
+// to the state precision, stored bin-major out[b][k][q] (4 slots per bin).
+// Block (q, b): vector q of instance b.
 template <typename Rl>
 __global__ void __launch_bounds__(256) pweight_dft_kernel(const double* wp, long long wp_bs, int P, void* out,
                                                           long long out_bs) {
@@ -210,8 +211,8 @@ __global__ void __launch_bounds__(256) pweight_dft_kernel(const double* wp, long
     x = y;
     y = t;
   }
-  cplx_t<Rl>* o = reinterpret_cast<cplx_t<Rl>*>(out) + (size_t)b * out_bs + (size_t)q * P;
-  for (int i = threadIdx.x; i < P; i += blockDim.x) o[i] = mk<cplx_t<Rl>>((Rl)x[i].x, (Rl)x[i].y);
+  cplx_t<Rl>* o = reinterpret_cast<cplx_t<Rl>*>(out) + (size_t)b * out_bs + q;  // [k][4] layout
+  for (int i = threadIdx.x; i < P; i += blockDim.x) o[(size_t)i * 4] = mk<cplx_t<Rl>>((Rl)x[i].x, (Rl)x[i].y);
 }
 
 cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P, int nb, void* out, long long out_bs,

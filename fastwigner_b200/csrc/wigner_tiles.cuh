@@ -26,6 +26,65 @@ __device__ __forceinline__ void factor_pair(const void* taba, const void* tabb, 
   eb = herm(eb, k, N);
 }
 
+// factor_pair for a column pair whose two entries are adjacent in a table
+// that starts on 16 bytes (taba = entry of column xa, xa even): one vector
+// load per bin.
+template <typename Rl, int N>
+__device__ __forceinline__ void factor_pair_vec(const void* taba, size_t tab_stride, int tab_real, const void* g,
+                                                int k, cplx_t<Rl>& ea, cplx_t<Rl>& eb) {
+  using C = cplx_t<Rl>;
+  const int kk = (k <= N / 2) ? k : N - k;
+  if constexpr (sizeof(Rl) == 4) {
+    if (tab_real) {
+      const float2 e = __ldg(reinterpret_cast<const float2*>(reinterpret_cast<const float*>(taba) + kk * tab_stride));
+      ea = mk<C>(e.x, 0.f);
+      eb = mk<C>(e.y, 0.f);
+    } else {
+      const float4 e = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(taba) + kk * tab_stride));
+      ea = mk<C>(e.x, e.y);
+      eb = mk<C>(e.z, e.w);
+    }
+  } else {
+    if (tab_real) {
+      const double2 e = __ldg(reinterpret_cast<const double2*>(reinterpret_cast<const double*>(taba) + kk * tab_stride));
+      ea = mk<C>(e.x, 0.0);
+      eb = mk<C>(e.y, 0.0);
+    } else {
+      ea = __ldg(reinterpret_cast<const C*>(taba) + kk * tab_stride);
+      eb = __ldg(reinterpret_cast<const C*>(taba) + kk * tab_stride + 1);
+    }
+  }
+  if (g != nullptr) {
+    const C gk = __ldg(reinterpret_cast<const C*>(g) + kk);
+    ea = cmul(ea, gk);
+    eb = cmul(eb, gk);
+  }
+  ea = herm(ea, k, N);
+  eb = herm(eb, k, N);
+}
+
+// The first n (<= MAXO) p-weight spectra at one bin ([k][q] layout, 4 entries,
+// 16-byte aligned): FP32 as one or two 16-byte loads.
+template <typename Rl>
+__device__ __forceinline__ void load_bin_weights(const cplx_t<Rl>* gk, int n, cplx_t<Rl> (&g)[4]) {
+  using C = cplx_t<Rl>;
+  if constexpr (sizeof(Rl) == 4) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(gk));
+    g[0] = mk<C>(a.x, a.y);
+    g[1] = mk<C>(a.z, a.w);
+    if (n > 2) {
+      const float4 b = __ldg(reinterpret_cast<const float4*>(gk) + 1);
+      g[2] = mk<C>(b.x, b.y);
+      g[3] = mk<C>(b.z, b.w);
+    } else {
+      g[2] = g[3] = mk<C>(0.f, 0.f);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) g[q] = q < n ? __ldg(gk + q) : mk<C>(0.0, 0.0);
+  }
+}
+
 // Spectral multiply between a forward and an inverse transform (shared by the
 // row and column passes).  v holds the natural-order spectrum Z of a + i b.
 // taba/tabb point at the half-spectrum factors of the two packed sequences;
@@ -179,10 +238,16 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
   for (int m = 0; m < RV; ++m) {
     const int k = j + m * T;
     C ea1, eb1, ea2, eb2;
-    factor_pair<Rl, N>(t1, t1 + esz, (size_t)X, a.tab_real, a.g1, k, ea1, eb1);
+    if (a.tab_vec) {
+      factor_pair_vec<Rl, N>(t1, (size_t)X, a.tab_real, a.g1, k, ea1, eb1);
+    } else {
+      factor_pair<Rl, N>(t1, t1 + esz, (size_t)X, a.tab_real, a.g1, k, ea1, eb1);
+    }
     if (same) {
       ea2 = ea1;
       eb2 = eb1;
+    } else if (a.tab_vec) {
+      factor_pair_vec<Rl, N>(t2, (size_t)X, a.tab_real, a.g2, k, ea2, eb2);
     } else {
       factor_pair<Rl, N>(t2, t2 + esz, (size_t)X, a.tab_real, a.g2, k, ea2, eb2);
     }
@@ -196,12 +261,13 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
         o.cb = Bi.y;
       }
       const Rl ur = A.x + Bi.y, ui = A.y - Bi.x;  // 2 x (spectrum a + spectrum b)
+      if (a.Mp > 0) {
+        C g[MAXO];
+        load_bin_weights<Rl>(G + (size_t)k * MAXO, a.Mp, g);
 #pragma unroll
-      for (int q = 0; q < MAXO; ++q)
-        if (q < a.Mp) {
-          const C g = __ldg(G + (size_t)q * N + k);
-          o.sq[q] += ur * g.x + ui * g.y;
-        }
+        for (int q = 0; q < MAXO; ++q)
+          if (q < a.Mp) o.sq[q] += ur * g[q].x + ui * g[q].y;
+      }
     }
     v[m] = cscale(cadd(cmul(A, ea2), cmul(Bi, eb2)), h);
   }

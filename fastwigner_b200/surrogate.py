@@ -62,11 +62,15 @@ def run_study(runs=200, nbeta=100, epochs=12, batch=16, grid=512, train_grid=128
         err = ((Ws - Wp).abs().amax(dim=(1, 2)).double() * dxdp).cpu().numpy()
         seed_only = sur.predict(Ds, As, beta)
         err_seed_only = ((seed_only - Wp).abs().amax(dim=(1, 2)).double() * dxdp).cpu().numpy()
+        st = setup.G // train_grid  # the same error on the training points only
+        err_seed_train = ((seed_only[:, ::st, ::st] - Wp[:, ::st, ::st]).abs().amax(dim=(1, 2)).double()
+                          * dxdp).cpu().numpy()
         del bb
         results.append(dict(beta=beta, instances=n_eval, plain_steps=n_plain, seeded_steps=n_seed,
                             plain_ms=ms_plain, seeded_ms=ms_seed, speedup=ms_plain / ms_seed,
                             max_err=float(err.max()), median_err=float(np.median(err)),
-                            surrogate_only_max_err=float(err_seed_only.max())))
+                            surrogate_only_max_err=float(err_seed_only.max()),
+                            surrogate_only_max_err_training_points=float(err_seed_train.max())))
         if log:
             log(json.dumps(results[-1]))
     return dict(data_seconds=t_data, train_seconds=t_train, final_loss=float(np.mean(losses[-50:])),
