@@ -1,7 +1,7 @@
 """Train the FNO surrogate on plain-Bloch thermal states and measure what it
 gains: wall time to a thermal state with and without the surrogate seed.
 
-    python -m fastwigner_b200.surrogate [--runs 200] [--epochs 12] [--out results.json]
+    python -m fastwigner_b200.surrogate [--runs 200] [--epochs 10] [--train-grid 256] [--out results.json]
 
 The workload is the Morse-oscillator thermal-state problem
 (V = D (1 - exp(-a (x - x_e)))^2, D ~ U(2, 10), a ~ U(0.5, 1.5),
@@ -32,8 +32,8 @@ def timed(fn):
     return out, e0.elapsed_time(e1)
 
 
-def run_study(runs=200, nbeta=100, epochs=12, batch=16, grid=512, train_grid=128, eval_betas=(5.0, 10.0, 20.0),
-              n_eval=16, refine_fraction=0.2, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
+def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256, eval_betas=(5.0, 10.0, 20.0),
+              n_eval=16, refine_fraction=0.15, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
               residual=True, log=print):
     rng = np.random.default_rng(seed)
     setup = MorseBlochSetup(grid=grid)
@@ -82,9 +82,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--runs", type=int, default=200)
     ap.add_argument("--nbeta", type=int, default=100)
-    ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--refine", type=float, default=0.2)
-    ap.add_argument("--train-grid", type=int, default=128)
+    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--refine", type=float, default=0.15)
+    ap.add_argument("--train-grid", type=int, default=256)
     ap.add_argument("--width", type=int, default=32)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--plain-target", action="store_true",
