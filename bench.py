@@ -75,6 +75,23 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(dist, x, device="cuda"):
+    """The largest per-rank value (device-timed milliseconds) on every rank."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(units_per_rank, steps, world, el_ms):
+    """Whole-job throughput of a weak-scaling run: every rank advanced
+    units_per_rank units for `steps` steps; the job took el_ms (max over ranks)."""
+    return units_per_rank * steps * world / (el_ms * 1e-3)
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clock / throttle-reason sampling during the timed region."""
@@ -237,13 +254,6 @@ def run_ours(args):
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # warm-up
     obs = torch.empty((max(args.steps, E2E_STEPS), B, 8), dtype=torch.float64, device="cuda")
     sim.propagate(args.warmup, obs=obs[: args.warmup])
@@ -261,9 +271,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     barrier()
     launches = lib.fw_launch_count() - n0
-    el_ms = max_over_ranks(start.elapsed_time(end))
+    el_ms = max_over_ranks(dist, start.elapsed_time(end))
     pts = GRID * GRID * B
-    value = pts * args.steps * world / (el_ms * 1e-3)
+    value = job_value(pts, args.steps, world, el_ms)
     # sanity: the states stay normalised and finite
     o = obs[args.steps - 1].cpu().numpy()
     finite = bool(np.isfinite(o).all())
@@ -300,8 +310,8 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = pts * E2E_STEPS * e2e_calls * world / (e2e_ms * 1e-3)
+    e2e_ms = max_over_ranks(dist, e0.elapsed_time(e1))
+    e2e_value = job_value(pts, E2E_STEPS * e2e_calls, world, e2e_ms)
     h2d = W0_pinned.numel() * 4 / E2E_STEPS
     d2h = (host_out.numel() * 4 + obs_host.numel() * 8) / E2E_STEPS
 
