@@ -217,11 +217,12 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   auto ring = [&](int k) { return plan->ring + (size_t)(k & 1) * ring_slot; };
   auto hist = [&](int k) { return d->obs_out == nullptr ? nullptr : d->obs_out + (size_t)k * B * M; };
 
-  // With a totals buffer, a small kernel after each column pass with partial
-  // sums reduces them per instance (and records the observable history); the
-  // next pass reads one total per instance.  Without it (fixed-scratch plans)
-  // every CTA of the next pass reduces the partials itself.
-  const bool totals = plan->tot != nullptr;
+  // With a totals buffer and a batch of 4 or more, a small kernel after each
+  // column pass with partial sums reduces them per instance (and records the
+  // observable history); the next pass reads one total per instance.  For
+  // smaller batches (where that launch would cost more than it saves) and for
+  // fixed-scratch plans every CTA of the next pass reduces the partials itself.
+  const bool totals = plan->tot != nullptr && B >= 4;
   auto col = [&](PassArgs a) -> int {
     a.tw = plan->twP;
     int np = 0;

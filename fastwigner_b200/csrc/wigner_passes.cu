@@ -90,10 +90,8 @@ template <> struct ColCfg<double, 4096> { static constexpr int T = 256, CP = 1, 
 
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
-template <typename Rl, int N>
-static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
-  using Cfg = RowCfg<Rl, N>;
-  constexpr int T = Cfg::T, G = Cfg::G, MINB = Cfg::MINB;
+template <typename Rl, int N, int T, int G, int MINB>
+static cudaError_t launch_row_cfg(const PassArgs& a, cudaStream_t st) {
   const size_t smem = (size_t)G * 2 * (N + N / 32) * sizeof(Rl);
   auto kern = row_pass_kernel<Rl, N, T, G, MINB>;
   static bool attr = false;
@@ -108,9 +106,13 @@ static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
 }
 
 template <typename Rl, int N>
-static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts) {
-  using Cfg = ColCfg<Rl, N>;
-  constexpr int T = Cfg::T, CP = Cfg::CP, MINB = Cfg::MINB;
+static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
+  using Cfg = RowCfg<Rl, N>;
+  return launch_row_cfg<Rl, N, Cfg::T, Cfg::G, Cfg::MINB>(a, st);
+}
+
+template <typename Rl, int N, int T, int CP, int MINB>
+static cudaError_t launch_col_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
   const size_t smem = col_ex_reals<Rl, N, T, CP>() * sizeof(Rl);
   auto kern = col_pass_kernel<Rl, N, T, CP, MINB>;
   static bool attr = false;
@@ -125,6 +127,13 @@ static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts)
   return cudaGetLastError();
 }
 
+template <typename Rl, int N>
+static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts) {
+  using Cfg = ColCfg<Rl, N>;
+  return launch_col_cfg<Rl, N, Cfg::T, Cfg::CP, Cfg::MINB>(a, st, nparts);
+}
+
+// Partial-sum records per instance of a plan's column passes: X / (2 CP).
 int col_parts(int dtype, int P, int X) {
   int cp = 0;
 #define CPV(R, N) if (P == N) cp = ColCfg<R, N>::CP;
