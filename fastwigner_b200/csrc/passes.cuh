@@ -96,11 +96,14 @@ __device__ __forceinline__ double prev_scale(const PassArgs& a, int b, double* r
   __syncthreads();
   const double tot = red[32];
   if (a.obs_hist != nullptr && first_tile) {
+    // one warp per column m: lanes sum records lane, lane+32, ...; fixed tree
     double* oh = a.obs_hist + (size_t)b * a.M;
-    for (int m = tid; m < a.M; m += nth) {
+    const int lane = tid & 31;
+    for (int m = tid >> 5; m < a.M; m += (nth + 31) >> 5) {
       double acc = 0.0;
-      for (int c = 0; c < a.prev_nparts; ++c) acc += __ldcg(pp + (size_t)c * a.M + m);
-      oh[m] = acc;
+      for (int c = lane; c < a.prev_nparts; c += 32) acc += __ldcg(pp + (size_t)c * a.M + m);
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) oh[m] = acc;
     }
   }
   return 1.0 / (tot * a.dxdp);
