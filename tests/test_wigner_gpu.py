@@ -177,3 +177,42 @@ def test_fp32_bloch_256():
     o.setup_bloch_fftw(kw["kT"], kw["dbeta"])
     o.get_gibbs_state_fftw()
     assert rel_l2(W, o.W) < FP32_TOL
+
+
+@pytest.mark.parametrize("P,X,precision", [(2048, 128, "float32"), (4096, 128, "float32"), (128, 4096, "float32"),
+                                           (1024, 128, "float64"), (2048, 128, "float64"), (4096, 128, "float64"),
+                                           (128, 4096, "float64")])
+def test_extreme_grid_shapes_match_oracle(P, X, precision):
+    """The largest transform lengths on either axis (each column / row pass
+    launch shape of the 2048- and 4096-point transforms) against the FP64 oracle."""
+    kw = dict(t=0.0, dt=0.005, X_gridDIM=X, X_amplitude=10.0, P_gridDIM=P, P_amplitude=10.0)
+    V = lambda x: 0.05 * x ** 4 - x ** 2  # noqa: E731
+    init = lambda x, p: np.exp(-(x + 1.3) ** 2 / 0.5 - 0.25 * (p - 0.4) ** 2) + 0 * x * p  # noqa: E731
+    q = fw().WignerMoyalFTTW1D(**kw, V=lambda _, x: V(x), K=lambda _, p: 0.5 * p * p,
+                               diff_V=lambda _, x: 0.2 * x ** 3 - 2 * x, diff_K=lambda _, p: p, precision=precision)
+    q.set_wignerfunction(lambda _, x, p: init(x, p))
+    W = q.propagate(10)
+    o = WignerOracle(**kw, V=V, K=lambda p: 0.5 * p * p, diff_V=lambda x: 0.2 * x ** 3 - 2 * x, diff_K=lambda p: p)
+    o.set_wignerfunction(init(o.X, o.P))
+    o.propagate(10)
+    if precision == "float64":
+        assert rel_l2(W, o.W) < FP64_TOL
+        for k in ("X_average", "P_average", "X_average_RHS", "P_average_RHS", "hamiltonian_average"):
+            np.testing.assert_allclose(getattr(q, k), getattr(o, k), rtol=FP64_TOL, atol=FP64_TOL)
+    else:
+        assert rel_l2(W, o.W) < FP32_TOL
+        for k in ("X_average", "P_average", "X_average_RHS"):
+            rtol, atol = FP32_OBS_TOL[k]
+            np.testing.assert_allclose(getattr(q, k), getattr(o, k), rtol=rtol, atol=atol)
+
+
+def test_zero_steps_leave_the_state_alone():
+    kw = dict(t=0.0, dt=0.01, X_gridDIM=128, X_amplitude=8.0, P_gridDIM=128, P_amplitude=7.0)
+    q = fw().WignerMoyalFTTW1D(**kw, V=lambda _, x: 0.5 * x * x, K=lambda _, p: 0.5 * p * p,
+                               diff_V=lambda _, x: x, diff_K=lambda _, p: p)
+    q.set_wignerfunction(lambda _, x, p: np.exp(-(x - 1) ** 2 - (p - 0.5) ** 2) + 0 * x * p)
+    W0 = np.array(q.wignerfunction, copy=True)
+    n0 = len(q.X_average)
+    W = q.propagate(0)
+    np.testing.assert_array_equal(np.asarray(W), W0)
+    assert q.t == 0.0 and len(q.X_average) == n0
