@@ -79,20 +79,30 @@ __device__ __forceinline__ void rho_prev_scale(const RhoArgs& a, int b, double* 
   sim = 0.0;
   if (a.prev_part == nullptr) return;
   const double* pp = a.prev_part + (size_t)b * a.prev_nparts * a.M;
-  if (threadIdx.x == 0) {
+  // lane-strided sums over the records and a fixed shuffle tree (deterministic,
+  // no serial chain through one thread); blockDim is a multiple of 32
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (warp == 0) {
     double tr = 0, ti = 0;
-    for (int c = 0; c < a.prev_nparts; ++c) {
+    for (int c = lane; c < a.prev_nparts; c += 32) {
       tr += pp[(size_t)c * a.M];
       ti += pp[(size_t)c * a.M + 1];
     }
-    red[0] = tr;
-    red[1] = ti;
+    for (int o = 16; o > 0; o >>= 1) {
+      tr += __shfl_xor_sync(0xffffffffu, tr, o);
+      ti += __shfl_xor_sync(0xffffffffu, ti, o);
+    }
+    if (lane == 0) {
+      red[0] = tr;
+      red[1] = ti;
+    }
   }
-  if (a.obs_hist != nullptr && blockIdx.x == 0) {
-    for (int m = threadIdx.x; m < a.M; m += blockDim.x) {
+  if (a.obs_hist != nullptr && blockIdx.x == 0) {  // one warp per record column
+    for (int m = warp; m < a.M; m += nw) {
       double acc = 0.0;
-      for (int c = 0; c < a.prev_nparts; ++c) acc += pp[(size_t)c * a.M + m];
-      a.obs_hist[(size_t)b * a.M + m] = acc;
+      for (int c = lane; c < a.prev_nparts; c += 32) acc += pp[(size_t)c * a.M + m];
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) a.obs_hist[(size_t)b * a.M + m] = acc;
     }
   }
   __syncthreads();
