@@ -180,33 +180,52 @@ __global__ void __launch_bounds__(G* T, MINB) rho_row_kernel(RhoArgs a) {
     double acc[4 + 2 * (2 * RMAXO)];
 #pragma unroll
     for (int q = 0; q < 4 + 4 * RMAXO; ++q) acc[q] = 0.0;
+    // per-thread sums over the row's RV elements in the state precision (the
+    // diagonal terms, one element per row, in FP64), then FP64 across threads
+    Rl s2 = 0;
+    Rl pr[RMAXO], pim[RMAXO];
+#pragma unroll
+    for (int q = 0; q < RMAXO; ++q) pr[q] = pim[q] = 0;
 #pragma unroll
     for (int m = 0; m < RV; ++m) {
       const int jj = j + m * T;
-      const double re = (double)v[m].x, im = (double)v[m].y;
-      acc[2] += re * re + im * im;
+      const Rl re = v[m].x, im = v[m].y;
+      s2 += re * re + im * im;
       if (jj == i) {
-        acc[0] += re;
-        acc[1] += im;
+        acc[0] += (double)re;
+        acc[1] += (double)im;
 #pragma unroll
         for (int q = 0; q < RMAXO; ++q)
           if (q < a.Mx) {
             const double wgt = __ldg(a.wx + (size_t)q * N + i);
-            acc[4 + 2 * q] += re * wgt;
-            acc[5 + 2 * q] += im * wgt;
+            acc[4 + 2 * q] += (double)re * wgt;
+            acc[5 + 2 * q] += (double)im * wgt;
           }
       }
 #pragma unroll
       for (int q = 0; q < RMAXO; ++q)
         if (q < a.Mp) {
           const double2 gk = __ldg(reinterpret_cast<const double2*>(a.gp) + (size_t)q * N + ((i - jj) & (N - 1)));
-          acc[4 + 2 * RMAXO + 2 * q] += re * gk.x - im * gk.y;
-          acc[5 + 2 * RMAXO + 2 * q] += re * gk.y + im * gk.x;
+          const Rl gx = (Rl)gk.x, gy = (Rl)gk.y;
+          pr[q] += re * gx - im * gy;
+          pim[q] += re * gy + im * gx;
         }
     }
+    acc[2] = (double)s2;
 #pragma unroll
-    for (int q = 0; q < 4 + 4 * RMAXO; ++q)
-      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    for (int q = 0; q < RMAXO; ++q) {
+      acc[4 + 2 * RMAXO + 2 * q] = (double)pr[q];
+      acc[5 + 2 * RMAXO + 2 * q] = (double)pim[q];
+    }
+    // level-major warp reduction of the accumulators in use (acc[3] stays 0)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int q = 0; q < 4 + 4 * RMAXO; ++q) {
+        const bool used = q < 3 || (q >= 4 && q < 4 + 2 * a.Mx) ||
+                          (q >= 4 + 2 * RMAXO && q < 4 + 2 * RMAXO + 2 * a.Mp);
+        if (used) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      }
     const int warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
