@@ -55,15 +55,17 @@ __device__ __forceinline__ double coord(int kind, int k, int N, double dX, doubl
 }
 
 // factor at element (i, j); row-constant parts may be precomputed by the caller
-template <typename Rl>
-__device__ __forceinline__ cplx_t<Rl> factor(const Factor& f, int i, int j, int N, double dX, double dP,
+// SH: the shear phase exp(i c coord_a(j) coord_b(i)) may be on (an FP64 sincos per
+// element); passes without shear are compiled without that code.
+template <typename Rl, bool SH>
+__device__ __forceinline__ cplx_t<Rl> factor_sh(const Factor& f, int i, int j, int N, double dX, double dP,
                                              const Rl* tab) {
   using C = cplx_t<Rl>;
   C r = mk<C>((Rl)f.s_re, (Rl)f.s_im);
   if (f.u) r = cmul(r, __ldg(reinterpret_cast<const C*>(f.u) + j));
   if (f.w) r = cmul(r, __ldg(reinterpret_cast<const C*>(f.w) + i));
   if (tab) r = cscale(r, __ldg(tab + (size_t)i * N + j));
-  if (f.shear_c != 0.0) {
+  if (SH && f.shear_c != 0.0) {
     const double ph = f.shear_c * coord<Rl>(f.shear_a, j, N, dX, dP) * coord<Rl>(f.shear_b, i, N, dX, dP);
     double sn, cs;
     sincos(ph, &sn, &cs);
@@ -113,22 +115,22 @@ __device__ __forceinline__ void rho_prev_scale(const RhoArgs& a, int b, double* 
   __syncthreads();
 }
 
-template <typename Rl, int N, int T, int RV>
+template <typename Rl, int N, int T, int RV, bool SH>
 __device__ __forceinline__ void apply_factor_row(cplx_t<Rl> (&v)[RV], const Factor& f, int i, int j0, double dX,
                                                  double dP, int b) {
   if (!f.on) return;
   const Rl* tab = f.tab ? reinterpret_cast<const Rl*>(f.tab) + (size_t)b * f.tab_bs : nullptr;
 #pragma unroll
-  for (int m = 0; m < RV; ++m) v[m] = cmul(v[m], factor<Rl>(f, i, j0 + m * T, N, dX, dP, tab));
+  for (int m = 0; m < RV; ++m) v[m] = cmul(v[m], factor_sh<Rl, SH>(f, i, j0 + m * T, N, dX, dP, tab));
 }
 
-template <typename Rl, int N, int T, int RV>
+template <typename Rl, int N, int T, int RV, bool SH>
 __device__ __forceinline__ void apply_factor_col(cplx_t<Rl> (&v)[RV], const Factor& f, int i0, int j, double dX,
                                                  double dP, int b) {
   if (!f.on) return;
   const Rl* tab = f.tab ? reinterpret_cast<const Rl*>(f.tab) + (size_t)b * f.tab_bs : nullptr;
 #pragma unroll
-  for (int m = 0; m < RV; ++m) v[m] = cmul(v[m], factor<Rl>(f, i0 + m * T, j, N, dX, dP, tab));
+  for (int m = 0; m < RV; ++m) v[m] = cmul(v[m], factor_sh<Rl, SH>(f, i0 + m * T, j, N, dX, dP, tab));
 }
 
 constexpr int RMAXO = 4;
@@ -150,7 +152,7 @@ __device__ __forceinline__ void transform(cplx_t<Rl> (&v)[RV], int dir, int j, E
 }
 
 // Row pass: G groups of T threads; group g owns row i.
-template <typename Rl, int N, int T, int G, int MINB>
+template <typename Rl, int N, int T, int G, int MINB, bool SH>
 __global__ void __launch_bounds__(G* T, MINB) rho_row_kernel(RhoArgs a) {
   using C = cplx_t<Rl>;
   constexpr int RV = N / T;
@@ -172,9 +174,9 @@ __global__ void __launch_bounds__(G* T, MINB) rho_row_kernel(RhoArgs a) {
   const C sc = mk<C>((Rl)sre, (Rl)sim);
 #pragma unroll
   for (int m = 0; m < RV; ++m) v[m] = cmul(R[j + m * T], sc);
-  apply_factor_row<Rl, N, T, RV>(v, a.f0, i, j, a.dX, a.dP, b);
+  apply_factor_row<Rl, N, T, RV, SH>(v, a.f0, i, j, a.dX, a.dP, b);
   transform<Rl, N, T, RV>(v, a.t1, j, ex, tw);
-  apply_factor_row<Rl, N, T, RV>(v, a.f1, i, j, a.dX, a.dP, b);
+  apply_factor_row<Rl, N, T, RV, SH>(v, a.f1, i, j, a.dX, a.dP, b);
   if (a.part_out != nullptr) {
     // [trace re, im, sum|rho|^2, 0, x-obs (re, im) x Mx, p-obs (re, im) x Mp]
     double acc[4 + 2 * (2 * RMAXO)];
@@ -243,9 +245,9 @@ __global__ void __launch_bounds__(G* T, MINB) rho_row_kernel(RhoArgs a) {
       a.part_out[((size_t)b * gridDim.x + blockIdx.x) * a.M + mo] = t;
     }
   }
-  apply_factor_row<Rl, N, T, RV>(v, a.f2, i, j, a.dX, a.dP, b);
+  apply_factor_row<Rl, N, T, RV, SH>(v, a.f2, i, j, a.dX, a.dP, b);
   transform<Rl, N, T, RV>(v, a.t2, j, ex, tw);
-  apply_factor_row<Rl, N, T, RV>(v, a.f3, i, j, a.dX, a.dP, b);
+  apply_factor_row<Rl, N, T, RV, SH>(v, a.f3, i, j, a.dX, a.dP, b);
 #pragma unroll
   for (int m = 0; m < RV; ++m) R[j + m * T] = v[m];
   if (a.sum_out != nullptr) {
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(G* T, MINB) rho_row_kernel(RhoArgs a) {
 }
 
 // Column pass: CP columns per CTA, T threads per column (interleaved exchange).
-template <typename Rl, int N, int T, int CP, int S, int MINB>
+template <typename Rl, int N, int T, int CP, int S, int MINB, bool SH>
 __global__ void __launch_bounds__(CP* T, MINB) rho_col_kernel(RhoArgs a) {
   using C = cplx_t<Rl>;
   constexpr int RV = N / T;
@@ -289,12 +291,12 @@ __global__ void __launch_bounds__(CP* T, MINB) rho_col_kernel(RhoArgs a) {
   const C sc = mk<C>((Rl)sre, (Rl)sim);
 #pragma unroll
   for (int m = 0; m < RV; ++m) v[m] = cmul(R[(size_t)(jt + m * T) * N + col], sc);
-  apply_factor_col<Rl, N, T, RV>(v, a.f0, jt, col, a.dX, a.dP, b);
+  apply_factor_col<Rl, N, T, RV, SH>(v, a.f0, jt, col, a.dX, a.dP, b);
   transform<Rl, N, T, RV>(v, a.t1, jt, ex, tw);
-  apply_factor_col<Rl, N, T, RV>(v, a.f1, jt, col, a.dX, a.dP, b);
-  apply_factor_col<Rl, N, T, RV>(v, a.f2, jt, col, a.dX, a.dP, b);
+  apply_factor_col<Rl, N, T, RV, SH>(v, a.f1, jt, col, a.dX, a.dP, b);
+  apply_factor_col<Rl, N, T, RV, SH>(v, a.f2, jt, col, a.dX, a.dP, b);
   transform<Rl, N, T, RV>(v, a.t2, jt, ex, tw);
-  apply_factor_col<Rl, N, T, RV>(v, a.f3, jt, col, a.dX, a.dP, b);
+  apply_factor_col<Rl, N, T, RV, SH>(v, a.f3, jt, col, a.dX, a.dP, b);
 #pragma unroll
   for (int m = 0; m < RV; ++m) R[(size_t)(jt + m * T) * N + col] = v[m];
 }
@@ -315,12 +317,16 @@ CCFG(double, 2048, 128, 2, 1) CCFG(double, 4096, 256, 2, 1)
 #undef RCFG
 #undef CCFG
 
-template <typename Rl, int N>
-static cudaError_t rho_row_n(const RhoArgs& a, cudaStream_t st, int* nparts) {
+static bool any_shear(const RhoArgs& a) {
+  return a.f0.shear_c != 0.0 || a.f1.shear_c != 0.0 || a.f2.shear_c != 0.0 || a.f3.shear_c != 0.0;
+}
+
+template <typename Rl, int N, bool SH>
+static cudaError_t rho_row_sh(const RhoArgs& a, cudaStream_t st, int* nparts) {
   using Cfg = RhoRowCfg<Rl, N>;
   constexpr int T = Cfg::T, G = Cfg::G, MINB = Cfg::MINB;
   const size_t smem = (size_t)G * 2 * (N + N / 32) * sizeof(Rl);
-  auto kern = rho_row_kernel<Rl, N, T, G, MINB>;
+  auto kern = rho_row_kernel<Rl, N, T, G, MINB, SH>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -333,13 +339,20 @@ static cudaError_t rho_row_n(const RhoArgs& a, cudaStream_t st, int* nparts) {
   return cudaGetLastError();
 }
 
+// Passes whose factors shear (the rho -> W transform) use the instantiation
+// with the per-element sincos; propagation passes carry none of that code.
 template <typename Rl, int N>
-static cudaError_t rho_col_n(const RhoArgs& a, cudaStream_t st) {
+static cudaError_t rho_row_n(const RhoArgs& a, cudaStream_t st, int* nparts) {
+  return any_shear(a) ? rho_row_sh<Rl, N, true>(a, st, nparts) : rho_row_sh<Rl, N, false>(a, st, nparts);
+}
+
+template <typename Rl, int N, bool SH>
+static cudaError_t rho_col_sh(const RhoArgs& a, cudaStream_t st) {
   using Cfg = RhoColCfg<Rl, N>;
   constexpr int T = Cfg::T, CP = Cfg::CP, MINB = Cfg::MINB;
   constexpr int S = ilog2_c(N / T > 32 ? 32 : N / T);
   const size_t smem = (size_t)2 * N * CP * sizeof(Rl);
-  auto kern = rho_col_kernel<Rl, N, T, CP, S, MINB>;
+  auto kern = rho_col_kernel<Rl, N, T, CP, S, MINB, SH>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -349,6 +362,11 @@ static cudaError_t rho_col_n(const RhoArgs& a, cudaStream_t st) {
   dim3 grid(N / CP, a.batch);
   kern<<<grid, CP * T, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+template <typename Rl, int N>
+static cudaError_t rho_col_n(const RhoArgs& a, cudaStream_t st) {
+  return any_shear(a) ? rho_col_sh<Rl, N, true>(a, st) : rho_col_sh<Rl, N, false>(a, st);
 }
 
 int rho_row_parts(int dtype, int N) {
