@@ -32,11 +32,132 @@ from __future__ import annotations
 
 import json
 import math
+import os
+import statistics
+import subprocess
+import threading
 
 import numpy as np
 import torch
 
 WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field")
+
+# NVML clock-event reason bits (nvmlClocksEventReason*): reported when active.
+_REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+
+
+class ClockSampler:
+    """SM clock and clock-event reasons sampled while a timed region runs.
+
+    Used as a context manager around the region: a thread reads NVML every
+    `interval` seconds from entry to exit (kernels run asynchronously, so the
+    host polls while the enqueued work executes, and even a region of a few
+    milliseconds gets samples).  Falls back to `nvidia-smi -lms 200` when NVML
+    is unavailable.  Only reads the GPU's state."""
+
+    SMI_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=None, interval=0.01):
+        self.device_index = torch.cuda.current_device() if device_index is None else device_index
+        self.interval = interval
+        self.sm, self.mx, self.reasons, self.source = [], [], set(), "unsampled"
+        self._stop = threading.Event()
+        self._thread = self._proc = self._nvml = self._handle = None
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        props = torch.cuda.get_device_properties(self.device_index)
+        try:
+            u = str(props.uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            pass
+        bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+        return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _sample_nvml(self):
+        nv, h = self._nvml, self._handle
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.sm.append(float(sm))
+        self.mx.append(float(mx))
+        self.reasons.update(n for n, b in _REASON_BITS.items() if bits & b)
+
+    def _loop(self):
+        while True:
+            try:
+                self._sample_nvml()
+            except Exception:
+                return
+            if self._stop.wait(self.interval):
+                return
+
+    def __enter__(self):
+        try:
+            self._handle = self._nvml_handle()
+            self._sample_nvml()
+            self.sm, self.mx, self.reasons = [], [], set()  # the entry sample only checks the handle
+            self.source = "nvml"
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._handle = None
+            try:
+                idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[self.device_index].strip() or str(
+                    self.device_index)
+            except IndexError:
+                idx = str(self.device_index)
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", idx, f"--query-gpu={self.SMI_QUERY}", "--format=csv,noheader,nounits",
+                     "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi"
+            except OSError:
+                self._proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+        if self._nvml is not None:
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                out, _ = self._proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+                out, _ = self._proc.communicate()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for ln in out.splitlines():
+                f = [c.strip() for c in ln.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm, mx = float(f[1]), float(f[2])
+                except ValueError:
+                    continue
+                self.sm.append(sm)
+                self.mx.append(mx)
+                self.reasons.update(n for n, v in zip(names, f[5:9]) if v.lower().startswith("active"))
+        return False
+
+    def summary(self):
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": max(self.mx), "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": self.source}
 
 
 def _peak():
@@ -49,16 +170,27 @@ def _peak():
         return 6650.0, "fallback hbm_gbs"
 
 
-def _timed(fn, warm=1):
+_last_clocks = {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+
+def _timed(fn, warm=2, reps=3):
+    """Median device time (ms) of `reps` calls of fn after `warm` untimed calls;
+    the SM clocks seen during the timed calls go into the workload's line."""
+    global _last_clocks
     for _ in range(warm):
         fn()
     torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    fn()
-    e.record()
-    torch.cuda.synchronize()
-    return s.elapsed_time(e)
+    out = []
+    with ClockSampler() as clk:
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            out.append(s.elapsed_time(e))
+    _last_clocks = clk.summary()
+    return float(np.median(out))
 
 
 def _line(name, value, unit, steps, ms, dtype, bytes_per_unit, config, extra=None):
@@ -68,7 +200,8 @@ def _line(name, value, unit, steps, ms, dtype, bytes_per_unit, config, extra=Non
             "value": value, "unit": unit, "n_gpus": 1, "steps": steps, "ms_per_step": ms / steps,
             "higher_is_better": True, "dtype": dtype, "data": "synthetic", "config": config,
             "roofline": {"bound": "hbm", "algorithmic_bytes_per_unit": bytes_per_unit, "achieved": gbs,
-                         "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_kind": kind}}
+                         "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_kind": kind},
+            "clocks": _last_clocks}
     if extra:
         line.update(extra)
     return line

@@ -7,6 +7,7 @@ travels with the source tree; it is rebuilt only when a source is newer.
 from __future__ import annotations
 
 import os
+import re
 import subprocess
 import sys
 from pathlib import Path
@@ -39,12 +40,33 @@ def _sources() -> list[Path]:
     return [CSRC / s for s in SOURCES if (CSRC / s).exists()]
 
 
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src: Path) -> set[Path]:
+    """src and every file it pulls in with #include "..." (recursively, any
+    extension: the translation units include .cu files as well as headers)."""
+    seen: set[Path] = set()
+    todo = [src.resolve()]
+    while todo:
+        f = todo.pop()
+        if f in seen or not f.exists():
+            continue
+        seen.add(f)
+        for name in _INCLUDE_RE.findall(f.read_text(errors="replace")):
+            for base in (f.parent, INCLUDE):
+                cand = (base / name).resolve()
+                if cand.exists():
+                    todo.append(cand)
+                    break
+    return seen
+
+
 def _stale(obj: Path, src: Path) -> bool:
     if not obj.exists():
         return True
-    deps = [src] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
     t = obj.stat().st_mtime
-    return any(d.stat().st_mtime > t for d in deps)
+    return any(d.stat().st_mtime > t for d in _deps(src))
 
 
 def build(verbose: bool = False, force: bool = False) -> Path:
