@@ -115,12 +115,13 @@ def profiled_traffic():
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(target_s, steps=None, grid=GRID):
-    """Time the FP64 oracle port (the reference algorithm, multi-threaded FFTs)
-    on one instance; returns (pt-steps/s, steps run, seconds, cores)."""
+def cpu_reference_rate(target_s, steps=None, grid=GRID, workers=None):
+    """Time the FP64 oracle port (the reference algorithm; FFTs on `workers`
+    threads, all host cores by default) on one instance; returns
+    (pt-steps/s, steps run, seconds, threads)."""
     from oracle.wigner_oracle import WignerOracle
 
-    cores = os.cpu_count() or 1
+    cores = workers or os.cpu_count() or 1
     o = WignerOracle(X_gridDIM=grid, X_amplitude=AMP, P_gridDIM=grid, P_amplitude=AMP, dt=DT,
                      V=V, K=K, diff_V=dV, diff_K=dK, fft_workers=cores)
     o.cache_exponents()
@@ -239,7 +240,8 @@ def run_ours(args):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tpp * pts) if tpp is not None else None,
                 "kernel": dom_kind, "kernel_ms": dom_ms, "col_ms": col_ms, "row_ms": row_ms,
-                "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs"}
+                "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
+                "frac_of_nominal_8000_gbs": achieved / 8000.0}
 
     # ---- end-to-end through the public API: pinned host states in, results out --
     e2e_calls = max(1, min(5, args.steps // E2E_STEPS))
@@ -268,6 +270,9 @@ def run_ours(args):
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"1 instance of the {GRID}x{GRID} workload, {csteps} FP64 steps in {cel:.1f} s "
                          f"(numpy restatement of WignerMoyalFTTW1D, scipy.fft workers={cores})"}
+        r1, s1, e1_, _ = cpu_reference_rate(args.cpu_seconds / 3, workers=1)
+        cpu["single_thread"] = {"value": r1, "unit": UNIT, "cores": 1,
+                                "sample": f"the same instance, {s1} FP64 steps in {e1_:.1f} s, scipy.fft workers=1"}
 
     if rank == 0:
         line = {
