@@ -135,6 +135,24 @@ __device__ __forceinline__ void apply_factor_col(cplx_t<Rl> (&v)[RV], const Fact
 
 constexpr int RMAXO = 4;
 
+// y if s else x, field by field (selects in registers; no copy of the kernel
+// parameters to local memory).
+__device__ __forceinline__ Factor pick_factor(bool s, const Factor& x, const Factor& y) {
+  Factor f;
+  f.on = s ? y.on : x.on;
+  f.s_re = s ? y.s_re : x.s_re;
+  f.s_im = s ? y.s_im : x.s_im;
+  f.u = s ? y.u : x.u;
+  f.w = s ? y.w : x.w;
+  f.tab = s ? y.tab : x.tab;
+  f.tab_bs = s ? y.tab_bs : x.tab_bs;
+  f.shear_c = s ? y.shear_c : x.shear_c;
+  f.shear_a = s ? y.shear_a : x.shear_a;
+  f.shear_b = s ? y.shear_b : x.shear_b;
+  f.sign = s ? y.sign : x.sign;
+  return f;
+}
+
 // forward (dir < 0) or unnormalised inverse (dir > 0) transform; the inverse is
 // conj(FFT(conj(x))) so each call site instantiates one transform.
 template <typename Rl, int N, int T, int RV, typename EX>
@@ -174,80 +192,85 @@ __global__ void __launch_bounds__(G* T, MINB) rho_row_kernel(RhoArgs a) {
   const C sc = mk<C>((Rl)sre, (Rl)sim);
 #pragma unroll
   for (int m = 0; m < RV; ++m) v[m] = cmul(R[j + m * T], sc);
-  apply_factor_row<Rl, N, T, RV, SH>(v, a.f0, i, j, a.dX, a.dP, b);
-  transform<Rl, N, T, RV>(v, a.t1, j, ex, tw);
-  apply_factor_row<Rl, N, T, RV, SH>(v, a.f1, i, j, a.dX, a.dP, b);
-  if (a.part_out != nullptr) {
-    // [trace re, im, sum|rho|^2, 0, x-obs (re, im) x Mx, p-obs (re, im) x Mp]
-    double acc[4 + 2 * (2 * RMAXO)];
+  // The two factor / transform / factor phases run as one loop body (not
+  // unrolled): the second phase executes the instructions the first one just
+  // fetched, which halves the straight-line code a one-wave launch streams
+  // through the instruction cache.  The observables belong to the first phase.
+#pragma unroll 1
+  for (int it = 0; it < 2; ++it) {
+    const bool second = it != 0;
+    apply_factor_row<Rl, N, T, RV, SH>(v, pick_factor(second, a.f0, a.f2), i, j, a.dX, a.dP, b);
+    transform<Rl, N, T, RV>(v, second ? a.t2 : a.t1, j, ex, tw);
+    apply_factor_row<Rl, N, T, RV, SH>(v, pick_factor(second, a.f1, a.f3), i, j, a.dX, a.dP, b);
+    if (!second && a.part_out != nullptr) {
+      // [trace re, im, sum|rho|^2, 0, x-obs (re, im) x Mx, p-obs (re, im) x Mp]
+      double acc[4 + 2 * (2 * RMAXO)];
 #pragma unroll
-    for (int q = 0; q < 4 + 4 * RMAXO; ++q) acc[q] = 0.0;
-    // per-thread sums over the row's RV elements in the state precision (the
-    // diagonal terms, one element per row, in FP64), then FP64 across threads
-    Rl s2 = 0;
-    Rl pr[RMAXO], pim[RMAXO];
+      for (int q = 0; q < 4 + 4 * RMAXO; ++q) acc[q] = 0.0;
+      // per-thread sums over the row's RV elements in the state precision (the
+      // diagonal terms, one element per row, in FP64), then FP64 across threads
+      Rl s2 = 0;
+      Rl pr[RMAXO], pim[RMAXO];
 #pragma unroll
-    for (int q = 0; q < RMAXO; ++q) pr[q] = pim[q] = 0;
+      for (int q = 0; q < RMAXO; ++q) pr[q] = pim[q] = 0;
 #pragma unroll
-    for (int m = 0; m < RV; ++m) {
-      const int jj = j + m * T;
-      const Rl re = v[m].x, im = v[m].y;
-      s2 += re * re + im * im;
-      if (jj == i) {
-        acc[0] += (double)re;
-        acc[1] += (double)im;
+      for (int m = 0; m < RV; ++m) {
+        const int jj = j + m * T;
+        const Rl re = v[m].x, im = v[m].y;
+        s2 += re * re + im * im;
+        if (jj == i) {
+          acc[0] += (double)re;
+          acc[1] += (double)im;
+#pragma unroll
+          for (int q = 0; q < RMAXO; ++q)
+            if (q < a.Mx) {
+              const double wgt = __ldg(a.wx + (size_t)q * N + i);
+              acc[4 + 2 * q] += (double)re * wgt;
+              acc[5 + 2 * q] += (double)im * wgt;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < RMAXO; ++q)
-          if (q < a.Mx) {
-            const double wgt = __ldg(a.wx + (size_t)q * N + i);
-            acc[4 + 2 * q] += (double)re * wgt;
-            acc[5 + 2 * q] += (double)im * wgt;
+          if (q < a.Mp) {
+            const double2 gk = __ldg(reinterpret_cast<const double2*>(a.gp) + (size_t)q * N + ((i - jj) & (N - 1)));
+            const Rl gx = (Rl)gk.x, gy = (Rl)gk.y;
+            pr[q] += re * gx - im * gy;
+            pim[q] += re * gy + im * gx;
           }
       }
+      acc[2] = (double)s2;
 #pragma unroll
-      for (int q = 0; q < RMAXO; ++q)
-        if (q < a.Mp) {
-          const double2 gk = __ldg(reinterpret_cast<const double2*>(a.gp) + (size_t)q * N + ((i - jj) & (N - 1)));
-          const Rl gx = (Rl)gk.x, gy = (Rl)gk.y;
-          pr[q] += re * gx - im * gy;
-          pim[q] += re * gy + im * gx;
-        }
-    }
-    acc[2] = (double)s2;
-#pragma unroll
-    for (int q = 0; q < RMAXO; ++q) {
-      acc[4 + 2 * RMAXO + 2 * q] = (double)pr[q];
-      acc[5 + 2 * RMAXO + 2 * q] = (double)pim[q];
-    }
-    // level-major warp reduction of the accumulators in use (acc[3] stays 0)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-      for (int q = 0; q < 4 + 4 * RMAXO; ++q) {
-        const bool used = q < 3 || (q >= 4 && q < 4 + 2 * a.Mx) ||
-                          (q >= 4 + 2 * RMAXO && q < 4 + 2 * RMAXO + 2 * a.Mp);
-        if (used) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      for (int q = 0; q < RMAXO; ++q) {
+        acc[4 + 2 * RMAXO + 2 * q] = (double)pr[q];
+        acc[5 + 2 * RMAXO + 2 * q] = (double)pim[q];
       }
-    const int warp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
+      // level-major warp reduction of the accumulators in use (acc[3] stays 0)
 #pragma unroll
-      for (int q = 0; q < 4 + 4 * RMAXO; ++q) ored[warp][q] = acc[q];
-    }
-    __syncthreads();
-    if ((int)threadIdx.x < a.M) {
-      const int mo = threadIdx.x;
-      int q;
-      if (mo < 4) q = mo;
-      else if (mo < 4 + 2 * a.Mx) q = mo;
-      else q = 4 + 2 * RMAXO + (mo - 4 - 2 * a.Mx);
-      double t = 0.0;
-      for (int w = 0; w < G * T / 32; ++w) t += ored[w][q];
-      a.part_out[((size_t)b * gridDim.x + blockIdx.x) * a.M + mo] = t;
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 4 + 4 * RMAXO; ++q) {
+          const bool used = q < 3 || (q >= 4 && q < 4 + 2 * a.Mx) ||
+                            (q >= 4 + 2 * RMAXO && q < 4 + 2 * RMAXO + 2 * a.Mp);
+          if (used) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        }
+      const int warp = threadIdx.x >> 5;
+      if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int q = 0; q < 4 + 4 * RMAXO; ++q) ored[warp][q] = acc[q];
+      }
+      __syncthreads();
+      if ((int)threadIdx.x < a.M) {
+        const int mo = threadIdx.x;
+        int q;
+        if (mo < 4) q = mo;
+        else if (mo < 4 + 2 * a.Mx) q = mo;
+        else q = 4 + 2 * RMAXO + (mo - 4 - 2 * a.Mx);
+        double t = 0.0;
+        for (int w = 0; w < G * T / 32; ++w) t += ored[w][q];
+        a.part_out[((size_t)b * gridDim.x + blockIdx.x) * a.M + mo] = t;
+      }
     }
   }
-  apply_factor_row<Rl, N, T, RV, SH>(v, a.f2, i, j, a.dX, a.dP, b);
-  transform<Rl, N, T, RV>(v, a.t2, j, ex, tw);
-  apply_factor_row<Rl, N, T, RV, SH>(v, a.f3, i, j, a.dX, a.dP, b);
 #pragma unroll
   for (int m = 0; m < RV; ++m) R[j + m * T] = v[m];
   if (a.sum_out != nullptr) {
