@@ -45,6 +45,40 @@ def integrate_field(E, t0, t1, pieces=4):
     return float(tot)
 
 
+def integrate_intervals(E, t0s, t1s, pieces):
+    """integrate_field(E, t0s[i], t1s[i], pieces) for every i, with E evaluated
+    on all quadrature nodes of all intervals in one call (same rule, same
+    order of operations); falls back to one call per interval when E does
+    not take arrays of any shape."""
+    t0s = np.asarray(t0s, dtype=np.float64)
+    t1s = np.asarray(t1s, dtype=np.float64)
+    edges = np.linspace(t0s, t1s, pieces + 1)             # (pieces + 1) x n
+    a, b = edges[:-1], edges[1:]
+    m, h = 0.5 * (a + b), 0.5 * (b - a)
+    nodes = m[..., None] + h[..., None] * _GL_X            # pieces x n x 8
+    try:
+        vals = np.asarray(E(nodes), dtype=np.float64)
+        if vals.shape != nodes.shape:
+            raise ValueError
+    except Exception:
+        return np.array([integrate_field(E, x, y, pieces) for x, y in zip(t0s, t1s)])
+    tot = np.zeros(t0s.shape)
+    for c in range(pieces):
+        tot += h[c] * np.sum(_GL_W * vals[c], axis=-1)
+    return tot
+
+
+def _on_times(f, times):
+    """float(f(t)) for every t: one call on the array when f vectorises."""
+    try:
+        v = np.asarray(f(times), dtype=np.float64)
+        if v.shape == times.shape:
+            return v
+    except Exception:
+        pass
+    return np.array([float(f(t)) for t in times])
+
+
 class StrongFieldWigner(WignerMoyalFTTW1D):
     """Keywords: the WignerMoyalFTTW1D grid keywords, ``V`` (static V0(self, x)),
     ``gauge`` ("velocity" or "length"), the field as ``A(self, t)`` (velocity)
@@ -107,6 +141,34 @@ class StrongFieldWigner(WignerMoyalFTTW1D):
         self._Aint = (t, a)
         return a
 
+    def vector_potentials(self, times):
+        """A at each of the increasing `times`, as successive vector_potential(t)
+        calls return it: the user's A on the whole array, else -int E advanced
+        interval by interval (the same composite Gauss-Legendre rule and piece
+        counts), with all intervals' quadrature nodes evaluated at once."""
+        times = np.asarray(times, dtype=np.float64)
+        if hasattr(self, "A"):
+            return _on_times(lambda t: self.A(t), times)
+        out = np.empty(times.shape)
+        out[0] = self.vector_potential(times[0])  # continues (or restarts) the cached integral
+        if times.size > 1:
+            t0s, t1s = times[:-1], times[1:]
+            pieces = np.maximum(1, np.ceil((t1s - t0s) / self.dt).astype(np.int64)) * 2
+            inc = np.empty(t0s.shape)
+            for pc in np.unique(pieces):
+                sel = np.nonzero(pieces == pc)[0]
+                inc[sel] = integrate_intervals(lambda u: self.E(u), t0s[sel], t1s[sel], int(pc))
+            out[:] = np.cumsum(np.concatenate(([out[0]], -inc)))  # a_k = a_(k-1) - int_k, in order
+            self._Aint = (float(times[-1]), float(out[-1]))
+        return out
+
+    def fields(self, times):
+        """E at each of `times` (one call on the array when E vectorises)."""
+        times = np.asarray(times, dtype=np.float64)
+        if hasattr(self, "E"):
+            return _on_times(lambda t: self.E(t), times)
+        return np.array([self.field(t) for t in times])
+
     def field(self, t):
         if hasattr(self, "E"):
             return float(self.E(t))
@@ -131,19 +193,20 @@ class StrongFieldWigner(WignerMoyalFTTW1D):
             return super()._propagate_chunk(nsteps, t0, tables, weights)
         times = t0 + self.dt * np.arange(1, nsteps + 1)
         tabV, tabK = self._static_tables()
-        h = self.hbar
         if self.gauge == "velocity":
-            A = np.array([self.vector_potential(t) for t in times])
+            A = self.vector_potentials(times)
             lam = self.Lambda.reshape(-1)
             g = np.exp(-1j * self.dt * np.outer(A, lam))             # exp(-i dt A(t) lambda)
             self._gK = torch.view_as_real(to_device(g, self._ct, self.device)).contiguous()
             self._gV = None
+            self._chunk_field = (A, np.zeros_like(A))
         else:
-            E = np.array([self.field(t) for t in times])
+            E = self.fields(times)
             th = self.Theta.reshape(-1)
             g = np.exp(0.5j * self.dt * np.outer(E, th))             # exp(i dt E(t) theta / 2)
             self._gV = torch.view_as_real(to_device(g, self._ct, self.device)).contiguous()
             self._gK = None
+            self._chunk_field = (np.zeros_like(E), E)
         return super()._propagate_chunk(nsteps, t0, tables=(tabV, 0, tabK, 0, False), weights=weights)
 
     def _chunk_steps(self):
@@ -160,16 +223,38 @@ class StrongFieldWigner(WignerMoyalFTTW1D):
         return wx, wp
 
     def _obs_weights(self, times):
+        """Static weights [x, V0'(x), V0(x)] and [p, p^2]: the field enters the
+        Ehrenfest observables only through the scalars A(t), E(t), applied to
+        the recorded sums afterwards (_expand_obs), so no per-step weights."""
         if not self.isEhrenfest:
             return None, None
-        pairs = [self._weights_at(t) for t in times]
-        wx = to_device(np.stack([a for a, _ in pairs]), torch.float64, self.device)
-        wp = to_device(np.stack([b for _, b in pairs]), torch.float64, self.device)
-        return wx, wp
+        if getattr(self, "_obs_static", None) is None:
+            X, P = self.X.reshape(-1), self.P.reshape(-1)
+            dv = np.broadcast_to(self.diff_V(self.X), self.X.shape).reshape(-1)
+            v = np.broadcast_to(self._v_at(self.X, self.t), self.X.shape).reshape(-1)
+            wx = to_device(np.stack([X, dv, v]), torch.float64, self.device)
+            wp = to_device(np.stack([P, P * P]), torch.float64, self.device)
+            self._obs_static = (wx, wp)
+        return self._obs_static
+
+    def _expand_obs(self, obs):
+        """Sums of the static weights -> the sums _weights_at(t) would give:
+        x, V0' + E, V0 + E x and p, p + A, (p + A)^2 / 2 (linear in the sums)."""
+        A, E = self._chunk_field
+        S, x1, dv, v, p1, p2 = (obs[:, c] for c in (0, 2, 3, 4, 5, 6))
+        full = np.empty((obs.shape[0], 8))
+        full[:, 0:2] = obs[:, 0:2]
+        full[:, 2] = x1
+        full[:, 3] = dv + E * S
+        full[:, 4] = v + E * x1
+        full[:, 5] = p1
+        full[:, 6] = p1 + A * S
+        full[:, 7] = 0.5 * p2 + A * p1 + 0.5 * A * A * S
+        return full
 
     def _ehrenfest_from_obs(self, obs):
         n = obs.shape[0]
-        super()._ehrenfest_from_obs(obs)
+        super()._ehrenfest_from_obs(self._expand_obs(obs))
         if self.gamma is not None:
             for k in range(len(self.X_average) - n, len(self.X_average)):
                 self.X_average_RHS[k] += self.gamma * (self.X_average_gibbs - self.X_average[k])
