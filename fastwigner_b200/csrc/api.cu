@@ -71,6 +71,7 @@ using namespace fw;
 
 struct fw_wigner_plan {
   int P, X, batch, dtype;
+  int small = 0;       // small-batch launch shapes (small_shapes)
   int nparts;          // column-pass CTAs per instance (partials per instance)
   void* twP = nullptr; // twiddles for length P
   void* twX = nullptr; // twiddles for length X
@@ -97,13 +98,14 @@ extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wign
     return fail(FW_EINVAL, "fw_wigner_plan_create: P_gridDIM and X_gridDIM must be powers of two in [128, 4096] (got " +
                                std::to_string(P) + " x " + std::to_string(X) + ")");
   if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_plan_create: batch must be in [1, 65535]");
-  const int np = col_parts(dtype, P, X);
+  const int small = small_shapes(dtype, P, X, batch);
+  const int np = col_parts(dtype, P, X, small);
   if (np <= 0) return fail(FW_EINVAL, "fw_wigner_plan_create: unsupported X for the column pass tile");
   fw_wigner_plan* p = new fw_wigner_plan();
-  p->P = P; p->X = X; p->batch = batch; p->dtype = dtype; p->nparts = np;
+  p->P = P; p->X = X; p->batch = batch; p->dtype = dtype; p->nparts = np; p->small = small;
   int rc = upload_twiddles(P, dtype, &p->twP);
   if (rc == FW_OK) rc = upload_twiddles(X, dtype, &p->twX);
-  if (rc == FW_OK) rc = upload_twiddles(X, dtype, &p->twsX, row_rv(dtype, X));
+  if (rc == FW_OK) rc = upload_twiddles(X, dtype, &p->twsX, row_rv(dtype, X, small));
   if (rc == FW_OK) {
     cudaError_t e = cudaMalloc(&p->ring, sizeof(double) * 2 * (size_t)batch * np * MMAX);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(partials)");
@@ -209,6 +211,7 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   base.s0_bs = d->s0_bstride;
   base.blend_c = d->blend_c;
   base.out_scale = 1.0;
+  base.small_shape = plan->small;
 
   auto tabV = [&](int k) { return advance(d->tabV, (long long)k * d->tabV_step, tes); };
   auto tabK = [&](int k) { return advance(d->tabK, (long long)k * d->tabK_step, tes); };
@@ -480,12 +483,13 @@ extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, c
   if (!size_supported(P) || !size_supported(X))
     return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: P and X must be powers of two in [128, 4096]");
   if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: batch must be in [1, 65535]");
-  const int np = col_parts(dtype, P, X);
+  const int small = small_shapes(dtype, P, X, batch);
+  const int np = col_parts(dtype, P, X, small);
   if (np <= 0) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: unsupported X for the column pass tile");
   const size_t rs = dtype == FW_F64 ? sizeof(double) : sizeof(float);
   const size_t twP_bytes = align256(2 * rs * (size_t)P);
   const size_t twX_bytes = align256(2 * rs * (size_t)X);
-  const int rvX = row_rv(dtype, X);
+  const int rvX = row_rv(dtype, X, small);
   const int nsX = stage_off(X, rvX, X);
   const size_t twsX_bytes = align256(2 * rs * (size_t)(nsX > 0 ? nsX : 1));
   const size_t ring_bytes = sizeof(double) * 2 * (size_t)batch * np * MMAX;
@@ -521,6 +525,7 @@ extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, c
   tmp.batch = batch;
   tmp.dtype = dtype;
   tmp.nparts = np;
+  tmp.small = small;
   tmp.twP = base;
   tmp.twX = base + twP_bytes;
   tmp.twsX = twsX;

@@ -13,8 +13,9 @@ cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P,
                                int dtype, cudaStream_t st);
 cudaError_t launch_totals(const double* part, int nparts, int M, int batch, double* tot, double* hist,
                           cudaStream_t st);
-int col_parts(int dtype, int P, int X);
-int row_rv(int dtype, int N);
+int col_parts(int dtype, int P, int X, int small);
+int row_rv(int dtype, int N, int small);
+int small_shapes(int dtype, int P, int X, int batch);
 bool size_supported(int n);
 
 void set_error(const std::string& msg);

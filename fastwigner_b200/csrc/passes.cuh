@@ -71,6 +71,9 @@ struct PassArgs {
   // totals_kernel, M doubles per instance): the input scale is read from
   // prev_tot[b*M] instead of reducing prev_part in every CTA.
   const double* prev_tot;
+  // launch shapes for small batches (RowCfgSmall / ColCfgSmall); decided once
+  // per plan, since the row twiddle table and the column record count follow it
+  int small_shape;
 };
 
 // Reduce previous-pass partial sums (per instance) into the input scale.

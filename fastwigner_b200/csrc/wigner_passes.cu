@@ -69,7 +69,7 @@ template <> struct RowCfg<float, 1024> { static constexpr int T = 32, G = 4, MIN
 template <> struct RowCfg<float, 2048> { static constexpr int T = 64, G = 4, MINB = 1; };
 template <> struct RowCfg<float, 4096> { static constexpr int T = 128, G = 2, MINB = 1; };
 template <> struct RowCfg<double, 128> { static constexpr int T = 16, G = 16, MINB = 1; };
-template <> struct RowCfg<double, 256> { static constexpr int T = 16, G = 16, MINB = 1; };
+template <> struct RowCfg<double, 256> { static constexpr int T = 16, G = 8, MINB = 2; };
 template <> struct RowCfg<double, 512> { static constexpr int T = 32, G = 8, MINB = 1; };
 template <> struct RowCfg<double, 1024> { static constexpr int T = 64, G = 4, MINB = 1; };
 template <> struct RowCfg<double, 2048> { static constexpr int T = 128, G = 2, MINB = 1; };
@@ -82,11 +82,21 @@ template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 8, MI
 template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 4, MINB = 1; };
 template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 2, MINB = 1; };
 template <> struct ColCfg<double, 128> { static constexpr int T = 16, CP = 16, MINB = 1; };
-template <> struct ColCfg<double, 256> { static constexpr int T = 16, CP = 16, MINB = 1; };
+template <> struct ColCfg<double, 256> { static constexpr int T = 16, CP = 8, MINB = 2; };
 template <> struct ColCfg<double, 512> { static constexpr int T = 32, CP = 8, MINB = 1; };
 template <> struct ColCfg<double, 1024> { static constexpr int T = 64, CP = 4, MINB = 1; };
 template <> struct ColCfg<double, 2048> { static constexpr int T = 128, CP = 2, MINB = 1; };
 template <> struct ColCfg<double, 4096> { static constexpr int T = 256, CP = 1, MINB = 1; };
+
+// Shapes for batches whose column pass would leave SMs idle with the shapes
+// above (the one-instance use of the drop-in classes): the same shapes unless
+// a sweep found faster ones for one instance.
+template <typename Rl, int N> struct RowCfgSmall : RowCfg<Rl, N> {};
+template <typename Rl, int N> struct ColCfgSmall : ColCfg<Rl, N> {};
+// FP64 256^2, one instance: 16.4 us per step vs 25.7 (at 512 instances the
+// shapes above are faster: 6.09e10 vs 4.82e10 pt-steps/s)
+template <> struct RowCfgSmall<double, 256> { static constexpr int T = 32, G = 4, MINB = 2; };
+template <> struct ColCfgSmall<double, 256> { static constexpr int T = 32, CP = 4, MINB = 2; };
 
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
@@ -107,6 +117,10 @@ static cudaError_t launch_row_cfg(const PassArgs& a, cudaStream_t st) {
 
 template <typename Rl, int N>
 static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
+  if (a.small_shape) {
+    using Cfg = RowCfgSmall<Rl, N>;
+    return launch_row_cfg<Rl, N, Cfg::T, Cfg::G, Cfg::MINB>(a, st);
+  }
   using Cfg = RowCfg<Rl, N>;
   return launch_row_cfg<Rl, N, Cfg::T, Cfg::G, Cfg::MINB>(a, st);
 }
@@ -129,14 +143,18 @@ static cudaError_t launch_col_cfg(const PassArgs& a, cudaStream_t st, int* npart
 
 template <typename Rl, int N>
 static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts) {
+  if (a.small_shape) {
+    using Cfg = ColCfgSmall<Rl, N>;
+    return launch_col_cfg<Rl, N, Cfg::T, Cfg::CP, Cfg::MINB>(a, st, nparts);
+  }
   using Cfg = ColCfg<Rl, N>;
   return launch_col_cfg<Rl, N, Cfg::T, Cfg::CP, Cfg::MINB>(a, st, nparts);
 }
 
 // Partial-sum records per instance of a plan's column passes: X / (2 CP).
-int col_parts(int dtype, int P, int X) {
+int col_parts(int dtype, int P, int X, int small) {
   int cp = 0;
-#define CPV(R, N) if (P == N) cp = ColCfg<R, N>::CP;
+#define CPV(R, N) if (P == N) cp = small ? ColCfgSmall<R, N>::CP : ColCfg<R, N>::CP;
   if (dtype == FW_F32) { CPV(float, 128) CPV(float, 256) CPV(float, 512) CPV(float, 1024) CPV(float, 2048) CPV(float, 4096) }
   else { CPV(double, 128) CPV(double, 256) CPV(double, 512) CPV(double, 1024) CPV(double, 2048) CPV(double, 4096) }
 #undef CPV
@@ -146,14 +164,23 @@ int col_parts(int dtype, int P, int X) {
 
 // Values per thread of the row pass transform of length N (the radix plan
 // its stage-layout twiddle table is built for).
-int row_rv(int dtype, int N) {
+int row_rv(int dtype, int N, int small) {
   int t = 0;
-#define RT(R, N_) if (N == N_) t = RowCfg<R, N_>::T;
+#define RT(R, N_) if (N == N_) t = small ? RowCfgSmall<R, N_>::T : RowCfg<R, N_>::T;
   if (dtype == FW_F32) { RT(float, 128) RT(float, 256) RT(float, 512) RT(float, 1024) RT(float, 2048) RT(float, 4096) }
   else { RT(double, 128) RT(double, 256) RT(double, 512) RT(double, 1024) RT(double, 2048) RT(double, 4096) }
 #undef RT
   return t > 0 ? N / t : 0;
 }
+// Small-batch shapes when the column pass with the regular shapes would have
+// fewer CTAs than the GPU has SMs.
+int small_shapes(int dtype, int P, int X, int batch) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int np = col_parts(dtype, P, X, 0);
+  return np > 0 && (long long)batch * np < sms ? 1 : 0;
+}
+
 bool size_supported(int n) { return n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096; }
 
 cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st) {

@@ -74,19 +74,23 @@ def test_graph_replay_equals_direct_launch_and_autotune_cache(tmp_path, monkeypa
         assert np.array_equal(Wa.cpu().numpy(), Wb.cpu().numpy())
 
 
-def test_uniform_batch_equals_single_instances():
+@pytest.mark.parametrize("B", [3, 12])
+def test_uniform_batch_equals_single_instances(B):
+    """FP64 256^2: a batch of 3 runs the small-batch launch shapes like the single
+    instances; a batch of 12 (192 column CTAs, more than the SMs) the regular ones,
+    so the two shape sets are checked against each other."""
     from fastwigner_b200 import WignerMoyalFTTW1D
     from fastwigner_b200.batch import WignerMoyalBatch
 
     V, K = dw(0.05, 1.0)
     kw = dict(X_gridDIM=256, X_amplitude=10.0, P_gridDIM=256, P_amplitude=10.0, dt=0.005)
-    b = WignerMoyalBatch(batch=3, **kw, V=V, K=K, diff_V=lambda x: 0.2 * x ** 3 - 2 * x, diff_K=lambda p: p,
+    b = WignerMoyalBatch(batch=B, **kw, V=V, K=K, diff_V=lambda x: 0.2 * x ** 3 - 2 * x, diff_K=lambda p: p,
                          precision="float64")
     rng = np.random.default_rng(1)
-    W0 = np.stack([np.exp(-(b.X - rng.uniform(-2, 2)) ** 2 - (b.P - rng.uniform(-1, 1)) ** 2) for _ in range(3)])
+    W0 = np.stack([np.exp(-(b.X - rng.uniform(-2, 2)) ** 2 - (b.P - rng.uniform(-1, 1)) ** 2) for _ in range(B)])
     b.set_wignerfunctions(W0)
     obs = b.propagate(12).cpu().numpy()
-    for i in range(3):
+    for i in range(B):
         q = WignerMoyalFTTW1D(**kw, t=0.0, V=lambda _, x: V(x), K=lambda _, p: K(p),
                               diff_V=lambda _, x: 0.2 * x ** 3 - 2 * x, diff_K=lambda _, p: p)
         q.set_wignerfunction(W0[i])
