@@ -180,11 +180,14 @@ def test_fp32_bloch_256():
 
 
 @pytest.mark.parametrize("P,X,precision", [(2048, 128, "float32"), (4096, 128, "float32"), (128, 4096, "float32"),
+                                           (1024, 2048, "float32"),
                                            (1024, 128, "float64"), (2048, 128, "float64"), (4096, 128, "float64"),
                                            (128, 4096, "float64")])
 def test_extreme_grid_shapes_match_oracle(P, X, precision):
     """The largest transform lengths on either axis (each column / row pass
-    launch shape of the 2048- and 4096-point transforms) against the FP64 oracle."""
+    launch shape of the 2048- and 4096-point transforms; 1024 x 2048 is the
+    strong-field grid, whose one-instance plan runs the small-batch row shape)
+    against the FP64 oracle."""
     kw = dict(t=0.0, dt=0.005, X_gridDIM=X, X_amplitude=10.0, P_gridDIM=P, P_amplitude=10.0)
     V = lambda x: 0.05 * x ** 4 - x ** 2  # noqa: E731
     init = lambda x, p: np.exp(-(x + 1.3) ** 2 / 0.5 - 0.25 * (p - 0.4) ** 2) + 0 * x * p  # noqa: E731
