@@ -126,6 +126,62 @@ class WignerMoyalBatch:
         self.t += steps * self.dt
         return obs
 
+    def propagate_host_batches(self, states, steps, out=None, obs_out=None):
+        """Propagate a sequence of host-resident batches (each B x P x X; pinned
+        CPU tensors copy asynchronously) by `steps` steps each, every batch from
+        the current time.  Batch i is copied in, normalised as by
+        set_wignerfunctions, propagated, and copied back to out[i] (host, same
+        shape) with its observable sums (steps x B x M) in obs_out[i] when given.
+        The copies in and out run on their own streams into two alternating
+        device state buffers, so they overlap the propagation of the
+        neighbouring batches.  out[i] may repeat tensors (the caller reuses
+        host buffers); everything is complete when the current stream is.
+        Afterwards self.W holds the last batch's final states.
+        Returns (out, obs_out)."""
+        n = len(states)
+        if out is None:
+            out = [torch.empty(self.W.shape, dtype=self._rt).pin_memory() for _ in range(n)]
+        if getattr(self, "_W_alt", None) is None or self._W_alt.shape != self.W.shape:
+            self._W_alt = torch.empty_like(self.W)
+        bufs = [self.W, self._W_alt]
+        obs_dev = [torch.empty((steps, self.batch, self._M), dtype=torch.float64, device=self.device)
+                   for _ in range(2)]
+        comp = torch.cuda.current_stream(self.device)
+        h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+        h2d.wait_stream(comp)  # earlier work on the buffers comes first
+        free = [None, None]    # per buffer: its last copy-out has finished
+        t0 = self.t
+        for i in range(n):
+            k = i & 1
+            buf = bufs[k]
+            with torch.cuda.stream(h2d):
+                if free[k] is not None:
+                    h2d.wait_event(free[k])
+                buf.copy_(states[i], non_blocking=True)
+                loaded = torch.cuda.Event()
+                loaded.record(h2d)
+            comp.wait_event(loaded)
+            s = buf.sum(dim=(1, 2), dtype=torch.float64) * self.dXdP
+            buf.div_(s.to(self._rt)[:, None, None])
+            self.W = buf
+            self.t = t0
+            self.propagate(steps, obs=obs_dev[k])
+            done = torch.cuda.Event()
+            done.record(comp)
+            with torch.cuda.stream(d2h):
+                d2h.wait_event(done)
+                out[i].copy_(buf, non_blocking=True)
+                if obs_out is not None:
+                    obs_out[i].copy_(obs_dev[k], non_blocking=True)
+                freed = torch.cuda.Event()
+                freed.record(d2h)
+            free[k] = freed
+        for ev in free:  # the last copies-out complete before the caller's stream moves on
+            if ev is not None:
+                comp.wait_event(ev)
+        self.t = t0 + steps * self.dt
+        return out, obs_out
+
     def propagate_timed(self, steps=1):
         """propagate() with per-launch CUDA-event times: returns (obs, ms[], kind[])."""
         obs = torch.empty((steps, self.batch, self._M), dtype=torch.float64, device=self.device)

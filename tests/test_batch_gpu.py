@@ -97,3 +97,35 @@ def test_uniform_batch_equals_single_instances(B):
         W = q.propagate(12)
         assert rel(b.W[i].cpu().numpy(), W) < 1e-12
         np.testing.assert_allclose(obs[:, i, 2] / obs[:, i, 0], q.X_average, rtol=1e-11)
+
+
+def test_host_batches_pipeline_equals_sequential_calls():
+    """propagate_host_batches (copies on their own streams, two alternating
+    device buffers) gives bit-identical states and observables to one
+    set_wignerfunctions + propagate call per host batch."""
+    import torch
+
+    from fastwigner_b200.batch import WignerMoyalBatch
+
+    V, K = dw(0.05, 1.0)
+    kw = dict(X_gridDIM=256, X_amplitude=10.0, P_gridDIM=256, P_amplitude=10.0, dt=0.005, V=V, K=K,
+              diff_V=lambda x: 0.2 * x ** 3 - 2 * x, diff_K=lambda p: p, precision="float32")
+    B, n, steps = 4, 5, 20
+    rng = np.random.default_rng(3)
+    a = WignerMoyalBatch(batch=B, **kw)
+    states = []
+    for _ in range(n):
+        W0 = np.stack([np.exp(-(a.X - rng.uniform(-2, 2)) ** 2 - (a.P - rng.uniform(-1, 1)) ** 2)
+                       for _ in range(B)]).astype(np.float32)
+        states.append(torch.from_numpy(W0).pin_memory())
+    obs_out = [torch.empty((steps, B, 8), dtype=torch.float64).pin_memory() for _ in range(n)]
+    out, _ = a.propagate_host_batches(states, steps, obs_out=obs_out)
+    torch.cuda.synchronize()
+    assert abs(a.t - steps * 0.005) < 1e-15
+    b = WignerMoyalBatch(batch=B, **kw)
+    for i in range(n):
+        b.set_wignerfunctions(states[i].cuda())
+        ob = b.propagate(steps)
+        np.testing.assert_array_equal(out[i].numpy(), b.W.cpu().numpy())
+        np.testing.assert_array_equal(obs_out[i].numpy(), ob.cpu().numpy())
+    np.testing.assert_array_equal(a.W.cpu().numpy(), out[-1].numpy())
