@@ -161,8 +161,10 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"moyal_double_well_{GRID}x{GRID}", "grid": [GRID, GRID], "dt": DT,
-                   "instances_per_step": 1, "implementation": "FP64 numpy restatement of WignerMoyalFTTW1D"},
+        "config": {"workload": f"moyal_double_well_{GRID}x{GRID}_batch{args.batch}", "grid": [GRID, GRID],
+                   "batch_per_gpu": args.batch, "dt": DT, "potential": "0.05 x^4 - x^2", "amplitudes": [AMP, AMP],
+                   "sample": f"one of the {args.batch} instances per step (the metric is per grid point)",
+                   "implementation": "FP64 numpy restatement of WignerMoyalFTTW1D"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
