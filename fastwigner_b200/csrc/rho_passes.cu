@@ -305,6 +305,7 @@ __global__ void __launch_bounds__(CP* T, MINB) rho_col_kernel(RhoArgs a) {
   rho_prev_scale(a, b, red, sre, sim);
   const int c = threadIdx.x % CP;
   const int jt = threadIdx.x / CP;
+  __builtin_assume(jt >= 0 && jt < T);  // launched with exactly CP * T threads
   const int col = blockIdx.x * CP + c;
   Rl* re = reinterpret_cast<Rl*>(smem_raw);
   ColEx<Rl, CP, S> ex{re, re + (size_t)N * CP, c};

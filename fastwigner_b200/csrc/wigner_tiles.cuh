@@ -344,6 +344,9 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
   const double sc = prev_scale(a, b, red, tile == 0);
   const int c = threadIdx.x % CP;
   const int j = threadIdx.x / CP;
+  // every launch of a column tile has exactly CP * T threads; telling the
+  // compiler lets it resolve which half of the spectrum bin k = j + m T lies in
+  __builtin_assume(j >= 0 && j < T);
   const int X = a.X;
   const int xa = tile * 2 * CP + 2 * c;
   Rl* re = reinterpret_cast<Rl*>(smem_raw);
