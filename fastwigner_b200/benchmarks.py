@@ -40,7 +40,8 @@ import threading
 import numpy as np
 import torch
 
-WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field")
+WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field", "rho_to_wigner_1024",
+             "moyal_absorbing_1024")
 
 # NVML clock-event reason bits (nvmlClocksEventReason*): reported when active.
 _REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
@@ -310,6 +311,53 @@ def strong_field(steps=500):
                  {"grid_x": 2048, "grid_p": 1024, "amplitudes": [200.0, 5.0], "dt": 0.05, "E0": E0, "omega": w,
                   "cycles": 8, "gamma": gamma, "kT": 0.1, "dbeta": 0.01, "gauge": "velocity", "passes_per_step": 3,
                   "l2_policy": "8 MiB state, L2-resident (effective figure)"})
+
+
+def rho_to_wigner_1024(reps=50):
+    """The rho -> W transform (three shear passes, the sign-flipped FFT, the
+    normalisation sum and scale) of the vn_1024 state, repeated."""
+    from .rho import RhoVNeumannCUDA1D
+
+    q = RhoVNeumannCUDA1D(X_gridDIM=1024, X_amplitude=10.0, dt=0.005, t=0.0, K="0.5 * P * P",
+                          V="0.05 * X * X * X * X - X * X", precision="float32")
+    rng = np.random.default_rng(7)
+    x0, p0 = rng.uniform(-2, 2), rng.uniform(-1, 1)
+    x = q.X.reshape(-1)
+    psi = np.exp(-((x - x0) ** 2) / (2 * 0.5 ** 2) + 1j * p0 * x)
+    q.set_rho(psi[:, None] * psi.conj()[None, :])
+    q.propagate(20)
+
+    def go():
+        for _ in range(reps):
+            q.get_wignerfunction()
+
+    ms = _timed(go)
+    n = 1024 * 1024
+    # copy (16) + 3 shear passes (48) + sign / FFT pass (16) + sum (8) + scale (16) + clone (16)
+    return _line("rho_to_wigner_1024", n * reps / (ms * 1e-3), "matrix-el/s", reps, ms, "c64", 120,
+                 {"grid": [1024, 1024], "transforms": reps, "passes": 6,
+                  "note": "one host read of the complex normalisation sum per transform",
+                  "l2_policy": "8 MiB matrix, L2-resident (effective figure)"},
+                 {"metric": "matrix elements transformed/sec", "ms_per_transform": ms / reps})
+
+
+def moyal_absorbing_1024(steps=400):
+    """WignerMoyalCUDA1D, FP32 1024^2 double well with the reference's x-p absorbing
+    mask (wigner_moyal_cuda_1d.py:39-44): the mask sits between the closing and
+    opening exp(V) half-steps, so the column pass runs its unfused form."""
+    from .wigner_cuda import WignerMoyalCUDA1D
+
+    q = WignerMoyalCUDA1D(X_gridDIM=1024, X_amplitude=10.0, P_gridDIM=1024, P_amplitude=10.0, dt=0.005, t=0.0,
+                          K="0.5 * P * P", V="0.05 * X * X * X * X - X * X", diff_K="P",
+                          diff_V="0.2 * X * X * X - 2.0 * X", precision="float32",
+                          abs_boundary_x_p="pow(abs(sin(0.5 * M_PI * (X + X_amplitude) / X_amplitude)), dt * 0.5)")
+    q.set_wignerfunction("exp(-(X - 1.0) * (X - 1.0) - 2.0 * P * P)")
+    ms = _timed(lambda: q.propagate(steps))
+    pts = 1024 * 1024
+    return _line("moyal_absorbing_1024", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 20,
+                 {"grid": [1024, 1024], "dt": 0.005, "boundary": "abs_boundary_x_p = |sin(pi (X + A) / 2A)|^(dt/2)",
+                  "passes_per_step": 2, "column_pass": "unfused (two transform pairs around the mask)",
+                  "l2_policy": "4 MiB state, L2-resident (effective figure)"})
 
 
 def run(name, **kw):
