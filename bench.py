@@ -12,7 +12,7 @@ passes per instance).  value = grid-point steps per second over all ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload {moyal_fp64_256,vn_1024,bloch_512,batch_uneven,strong_field,
-                                rho_to_wigner_1024,moyal_absorbing_1024}
+                                strong_field_frames,rho_to_wigner_1024,moyal_absorbing_1024}
 
 Under torchrun (N > 1) every rank advances its own batch (different seeds,
 no data-path collective): weak scaling, time = max over ranks.

@@ -40,8 +40,8 @@ import threading
 import numpy as np
 import torch
 
-WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field", "rho_to_wigner_1024",
-             "moyal_absorbing_1024")
+WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field", "strong_field_frames",
+             "rho_to_wigner_1024", "moyal_absorbing_1024")
 
 # NVML clock-event reason bits (nvmlClocksEventReason*): reported when active.
 _REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
@@ -291,7 +291,7 @@ def batch_uneven(steps=2000, n=256):
                  {"status": sim.status()})
 
 
-def strong_field(steps=500):
+def _strong_field_sim():
     from .strong_field import StrongFieldWigner
 
     rng = np.random.default_rng(5)
@@ -305,12 +305,42 @@ def strong_field(steps=500):
                           V=lambda _, x: -1.0 / np.sqrt(x * x + 1.0), diff_V=lambda _, x: x / (x * x + 1.0) ** 1.5,
                           gauge="velocity", E=E, gamma=gamma, kT=0.1, dbeta=0.01, precision="float32")
     q.set_wignerfunction(q.gibbs_state)
+    return q, E0, w, gamma
+
+
+def strong_field(steps=500):
+    q, E0, w, gamma = _strong_field_sim()
     ms = _timed(lambda: q.propagate(steps))
     pts = 2048 * 1024
     return _line("strong_field", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 32,
                  {"grid_x": 2048, "grid_p": 1024, "amplitudes": [200.0, 5.0], "dt": 0.05, "E0": E0, "omega": w,
                   "cycles": 8, "gamma": gamma, "kT": 0.1, "dbeta": 0.01, "gauge": "velocity", "passes_per_step": 3,
                   "l2_policy": "8 MiB state, L2-resident (effective figure)"})
+
+
+def strong_field_frames(steps=500, every=20):
+    """strong_field with the Wigner function recorded every `every` steps
+    through a FrameRecorder (propagate(steps, frames=..., frame_every=...):
+    device snapshot on the compute stream, pinned-host copy on a side stream,
+    4-slot ring, no wait between frames), all frames drained to host arrays
+    inside the timed region; the plain run is timed beside it."""
+    from .results import FrameRecorder
+
+    q = _strong_field_sim()[0]
+    rec = FrameRecorder(depth=4)
+
+    def go():
+        q.propagate(steps, frames=rec, frame_every=every)
+        return rec.take()
+
+    ms = _timed(go)
+    plain = _timed(lambda: q.propagate(steps))
+    pts = 2048 * 1024
+    nf = steps // every
+    return _line("strong_field_frames", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 32,
+                 {"grid_x": 2048, "grid_p": 1024, "frames": nf, "frame_every": every,
+                  "frame_bytes": pts * 4, "ring_depth": 4},
+                 {"plain_ms_per_step": plain / steps, "frame_overhead": ms / plain - 1.0})
 
 
 def rho_to_wigner_1024(reps=50):

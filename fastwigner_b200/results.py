@@ -49,8 +49,9 @@ class FrameRecorder:
     ``record(t=..., wigner=tensor, prob=tensor)`` snapshots the device tensors
     into the next slot of a ring of ``depth`` device buffers on the caller's
     stream (an HBM copy, ordered with the propagation, so the caller may go on
-    updating the tensors at once), then copies the snapshot into that slot's
-    pinned host buffers on a side stream and returns without waiting.  When
+    updating the tensors at once), then copies the snapshot into pinned host
+    buffers of its own (torch's caching host allocator) on a side stream and
+    returns without waiting; the frames hand those buffers out as numpy arrays.  When
     the ring wraps, the oldest slot's copy is waited for and the frame moved
     to the frame list.  ``frames()`` drains the ring; ``save(path,
     **settings)`` writes one ``.npz``: ``settings_<key>`` entries and
@@ -68,10 +69,13 @@ class FrameRecorder:
         if slot.get("event") is None:
             return
         slot["event"].synchronize()
-        frame = {k: v.numpy().copy() for k, v in slot["host"].items()}
+        # each frame owns its pinned buffers (from torch's caching host
+        # allocator): hand them out as numpy views, no host copy
+        frame = {k: v.numpy() for k, v in slot["host"].items()}
         frame.update(slot["scalars"])
         self._done.append((slot["index"], frame))
         slot["event"] = None
+        slot["host"] = {}
 
     @staticmethod
     def _fit(store, k, v, **kw):
@@ -101,7 +105,8 @@ class FrameRecorder:
             self._stream.wait_stream(torch.cuda.current_stream())
             with torch.cuda.stream(self._stream):
                 for k, v in tensors.items():
-                    self._fit(host, k, v, pin_memory=True).copy_(dev[k], non_blocking=True)
+                    host[k] = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                    host[k].copy_(dev[k], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(self._stream)
             slot.update(event=ev, scalars=scalars, index=self._count)
@@ -118,6 +123,13 @@ class FrameRecorder:
             self._retire(slot)
         self._done.sort(key=lambda f: f[0])
         return [f for _, f in self._done]
+
+    def take(self):
+        """frames(), after which the recorder forgets them (its buffers stay
+        allocated for the next frames): for long runs drained in pieces."""
+        out = self.frames()
+        self._done = []
+        return out
 
     def save(self, path, **settings):
         out = {f"settings_{k}": np.asarray(v) for k, v in settings.items()}

@@ -188,9 +188,9 @@ class StrongFieldWigner(WignerMoyalFTTW1D):
     def _tables_static(self):
         return True
 
-    def _propagate_chunk(self, nsteps, t0, tables=None, weights=None):
+    def _propagate_chunk(self, nsteps, t0, tables=None, weights=None, host=True):
         if tables is not None:
-            return super()._propagate_chunk(nsteps, t0, tables, weights)
+            return super()._propagate_chunk(nsteps, t0, tables, weights, host=host)
         times = t0 + self.dt * np.arange(1, nsteps + 1)
         tabV, tabK = self._static_tables()
         if self.gauge == "velocity":
@@ -207,10 +207,16 @@ class StrongFieldWigner(WignerMoyalFTTW1D):
             self._gV = torch.view_as_real(to_device(g, self._ct, self.device)).contiguous()
             self._gK = None
             self._chunk_field = (np.zeros_like(E), E)
-        return super()._propagate_chunk(nsteps, t0, tables=(tabV, 0, tabK, 0, False), weights=weights)
+        return super()._propagate_chunk(nsteps, t0, tables=(tabV, 0, tabK, 0, False), weights=weights, host=host)
+
+    def _chunk_context(self):
+        return getattr(self, "_chunk_field", None)
+
+    def _set_chunk_context(self, ctx):
+        self._chunk_field = ctx
 
     def _chunk_steps(self):
-        return 4096
+        return 64  # field factors for 64 steps are built while the previous 64 run
 
     def _weights_at(self, t):
         X, P = self.X.reshape(-1), self.P.reshape(-1)

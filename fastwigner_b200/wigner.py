@@ -228,8 +228,9 @@ class _WignerBase:
         return self._W
 
     # -- propagation ------------------------------------------------------------
-    def _propagate_chunk(self, nsteps, t0, tables=None, weights=None):
-        """Run nsteps steps starting after time t0; return the observable sums (nsteps x M).
+    def _propagate_chunk(self, nsteps, t0, tables=None, weights=None, host=True):
+        """Run nsteps steps starting after time t0; return the observable sums
+        (nsteps x M; a numpy copy, or the device tensor when host is False).
 
         tables: optional (tabV, vstep, tabK, kstep, tab_real) overriding the
         Hamiltonian's phase tables; weights: optional (wx, wp) overriding the
@@ -279,7 +280,15 @@ class _WignerBase:
         check(self._lib.fw_wigner_propagate(self._plan, _lib.ctypes.byref(d), nsteps, stream_handle()),
               "fw_wigner_propagate")
         self._host_cache = None
-        return obs.cpu().numpy()
+        return obs.cpu().numpy() if host else obs
+
+    def _chunk_context(self):
+        """Host-side state of the last chunk that _ehrenfest_from_obs needs, for
+        chunks whose observables are processed later (propagate with frames)."""
+        return None
+
+    def _set_chunk_context(self, ctx):
+        pass
 
     def _td_tables(self, times, which):
         td = self._v_time_dependent() if which == "V" else self._k_time_dependent()
@@ -309,19 +318,37 @@ class _WignerBase:
         per = (self.X_minus.size + self.P_plus.size) * (8 if not self._f64 else 16)
         return max(1, _TD_CHUNK_BYTES // per)
 
-    def propagate(self, steps=1):
+    def propagate(self, steps=1, frames=None, frame_every=0):
         """Advance by `steps` time steps, renormalising and recording the
-        Ehrenfest observables after each (wigner_moyal_fftw_1d.py:418-440)."""
+        Ehrenfest observables after each (wigner_moyal_fftw_1d.py:418-440).
+
+        The steps run in chunks (per-step tables or factor vectors are built on
+        the host one chunk at a time) without waiting for the device between
+        chunks, so the host prepares a chunk while the previous one runs; the
+        Ehrenfest lists are filled from every chunk's sums before returning.
+
+        Extension: with a FrameRecorder `frames` and frame_every = k > 0 the
+        state is recorded (``frames.record(t=..., wigner=<device state>)``)
+        after every k steps."""
         steps = int(steps)
+        every = int(frame_every) if frames is not None else 0
         done = 0
+        pending = []
         while done < steps:
             n = min(steps - done, self._chunk_steps())
-            obs = self._propagate_chunk(n, self.t)
+            if every > 0:
+                n = min(n, every - done % every)
+            pending.append((self._propagate_chunk(n, self.t, host=False), self._chunk_context()))
             self.t += n * self.dt
+            done += n
+            if every > 0 and done % every == 0:
+                frames.record(t=self.t, wigner=self.wigner_device)
+        for obs, ctx in pending:
+            obs = obs.cpu().numpy()
+            self._set_chunk_context(ctx)
             self._last_obs = obs
             if self.isEhrenfest:
                 self._ehrenfest_from_obs(obs)
-            done += n
         return self._returned_state()
 
     def single_step_propagation(self):

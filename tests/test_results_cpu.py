@@ -46,3 +46,20 @@ def test_frame_recorder_host_tensors(tmp_path):
     z = np.load(p)
     assert z["settings_dt"] == 0.05
     np.testing.assert_array_equal(z["frame4_wigner"], fr[4]["wigner"])
+
+
+def test_frame_recorder_take_drains_in_pieces():
+    rec = FrameRecorder(depth=2)
+    W = torch.zeros(2, 2)
+    for i in range(3):
+        W += 1
+        rec.record(t=i, wigner=W)
+    first = rec.take()
+    assert [f["t"] for f in first] == [0, 1, 2]
+    assert rec.frames() == []
+    for i in range(3, 5):
+        W += 1
+        rec.record(t=i, wigner=W)
+    second = rec.take()
+    assert [f["t"] for f in second] == [3, 4]
+    np.testing.assert_array_equal(second[-1]["wigner"], np.full((2, 2), 5.0, dtype=np.float32))
