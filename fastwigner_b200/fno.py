@@ -392,6 +392,39 @@ def generate_dataset(setup, n_runs, betas, rng, train_grid=128, chunk_runs=64):
     return P, S
 
 
+def allreduce_mean_(tensors, group=None):
+    """Average each tensor over the ranks of `group` in place: one flat buffer,
+    one all_reduce (NCCL on GPU tensors, gloo on CPU ones)."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    if world == 1 or not tensors:
+        return
+    flat = torch.cat([t.reshape(-1) for t in tensors])
+    dist.all_reduce(flat, group=group)
+    flat /= world
+    off = 0
+    for t in tensors:
+        n = t.numel()
+        t.view(-1).copy_(flat[off:off + n])
+        off += n
+
+
+def dp_steps_per_epoch(local_n, batch, group=None):
+    """Optimizer steps per epoch when every rank trains on its own local_n
+    samples: the smallest local_n // batch over the ranks, so that all ranks
+    take the same steps (and the same gradient all-reduces)."""
+    n = local_n // batch
+    if group is None:
+        return n
+    import torch.distributed as dist
+
+    t = torch.tensor([n], dtype=torch.int64,
+                     device="cuda" if dist.get_backend(group) == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
+    return int(t.item())
+
+
 def normalise_params(P):
     """(D, a, beta) -> network inputs: D/10, a, log(beta)/log(20)."""
     P = np.asarray(P, dtype=np.float64)
@@ -427,8 +460,13 @@ class BlochSurrogate:
         B = torch.exp(-c[:, None, None] * (Hh - Hh.amin(dim=(1, 2), keepdim=True)))
         return (B / B.sum(dim=(1, 2), keepdim=True)).float()
 
-    def train(self, P, S, epochs=20, batch=16, lr=2e-3, rng=None, log=None):
-        """P: (N, 3) raw (D, a, beta); S: (N, g, g) states (normalised to unit sum)."""
+    def train(self, P, S, epochs=20, batch=16, lr=2e-3, rng=None, log=None, group=None):
+        """P: (N, 3) raw (D, a, beta); S: (N, g, g) states (normalised to unit sum).
+
+        group: a torch.distributed process group for data-parallel training;
+        every rank passes its own samples (P, S) and the same initial
+        parameters, and the gradients are averaged over the ranks before each
+        Adam step (one all_reduce), so the parameters stay identical."""
         rng = rng or np.random.default_rng(0)
         X = normalise_params(P)
         N = len(X)
@@ -440,16 +478,19 @@ class BlochSurrogate:
             for c0 in range(0, N, 512):
                 B = self.baseline(P[c0:c0 + 512], full=False)
                 T[c0:c0 + 512] = (S[c0:c0 + 512] - B) / B.amax(dim=(1, 2), keepdim=True)
-        steps = epochs * (N // batch)
+        per_epoch = dp_steps_per_epoch(N, batch, group)
+        steps = epochs * per_epoch
         losses = []
         it = 0
         for ep in range(epochs):
             perm = rng.permutation(N)
-            for b0 in range(0, N - batch + 1, batch):
+            for b0 in range(0, per_epoch * batch, batch):
                 idx = perm[b0:b0 + batch]
                 lr_t = lr * 0.5 * (1 + math.cos(math.pi * it / max(1, steps)))
                 loss, dY = self.net.loss_and_grad(X[idx], self.xs_t, self.ps_t, T[torch.as_tensor(idx)])
                 self.net.backward(dY)
+                if group is not None:
+                    allreduce_mean_([self.net.grads[k] for k in self.net.names], group)
                 self.net.adam_step(lr_t)
                 losses.append(loss)
                 it += 1

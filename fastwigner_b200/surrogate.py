@@ -2,6 +2,7 @@
 gains: wall time to a thermal state with and without the surrogate seed.
 
     python -m fastwigner_b200.surrogate [--runs 200] [--epochs 10] [--train-grid 256] [--out results.json]
+    torchrun --nproc-per-node N -m fastwigner_b200.surrogate --dp ...   # data-parallel training
 
 The workload is the Morse-oscillator thermal-state problem
 (V = D (1 - exp(-a (x - x_e)))^2, D ~ U(2, 10), a ~ U(0.5, 1.5),
@@ -32,22 +33,39 @@ def timed(fn):
     return out, e0.elapsed_time(e1)
 
 
+def local_runs(runs, world, rank):
+    """Plain-Bloch runs generated by `rank` when `runs` are shared by `world`
+    data-parallel ranks (the first runs % world ranks take one more)."""
+    return runs // world + (1 if rank < runs % world else 0)
+
+
 def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256, eval_betas=(5.0, 10.0, 20.0),
               n_eval=16, refine_fraction=0.15, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
-              residual=True, log=print):
-    rng = np.random.default_rng(seed)
+              residual=True, log=print, group=None):
+    """group: a process group for data-parallel training -- each rank
+    generates its share of the runs (its own seed), the network starts from
+    the same seed everywhere and the gradients are averaged before every step;
+    rank 0 alone evaluates and returns the results (the others return None)."""
+    world, rank = 1, 0
+    if group is not None:
+        import torch.distributed as dist
+
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+    rng = np.random.default_rng(seed + 7919 * rank)
     setup = MorseBlochSetup(grid=grid)
     betas = np.exp(np.linspace(np.log(0.1), np.log(20.0), nbeta))
     t0 = time.time()
-    P, S = generate_dataset(setup, runs, betas, rng, train_grid=train_grid)
+    P, S = generate_dataset(setup, local_runs(runs, world, rank), betas, rng, train_grid=train_grid)
     t_data = time.time() - t0
     net = FNO2d(n_params=3, width=width, modes=modes, layers=layers, proj=128, seed=seed)
     sur = BlochSurrogate(setup, net, train_grid=train_grid, residual=residual)
     t0 = time.time()
-    losses = sur.train(P, S, epochs=epochs, batch=batch, lr=lr, rng=rng,
-                       log=(lambda ep, l: log(f"epoch {ep}: loss {l:.3e}")) if log else None)
+    losses = sur.train(P, S, epochs=epochs, batch=batch, lr=lr, rng=rng, group=group,
+                       log=(lambda ep, l: log(f"epoch {ep}: loss {l:.3e}")) if (log and rank == 0) else None)
     torch.cuda.synchronize()
     t_train = time.time() - t0
+    if rank != 0:
+        return None
     dxdp = setup.dX * setup.dP
     results = []
     for beta in eval_betas:
@@ -74,8 +92,8 @@ def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256
         if log:
             log(json.dumps(results[-1]))
     return dict(data_seconds=t_data, train_seconds=t_train, final_loss=float(np.mean(losses[-50:])),
-                samples=int(len(P)), epochs=epochs, residual=residual, train_grid=train_grid, width=width,
-                refine_fraction=refine_fraction, results=results)
+                samples=int(len(P)) * world, ranks=world, epochs=epochs, residual=residual,
+                train_grid=train_grid, width=width, refine_fraction=refine_fraction, results=results)
 
 
 def main():
@@ -91,14 +109,35 @@ def main():
                     help="learn the thermal state itself instead of the correction to the harmonic baseline")
     ap.add_argument("--eval-betas", default="5,10,20")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--dp", action="store_true",
+                    help="data-parallel training, one process per GPU under torchrun (NCCL gradient all-reduce)")
     a = ap.parse_args()
-    r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine, train_grid=a.train_grid,
-                  width=a.width, lr=a.lr, residual=not a.plain_target,
-                  eval_betas=tuple(float(b) for b in a.eval_betas.split(",")))
-    print(json.dumps(r))
-    if a.out:
-        with open(a.out, "w") as f:
-            json.dump(r, f, indent=1)
+    group = None
+    if a.dp:
+        import datetime
+        import os
+
+        import torch.distributed as dist
+
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        group = dist.group.WORLD
+    try:
+        r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine,
+                      train_grid=a.train_grid, width=a.width, lr=a.lr, residual=not a.plain_target,
+                      eval_betas=tuple(float(b) for b in a.eval_betas.split(",")), group=group)
+    finally:
+        if group is not None:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if r is not None:
+        print(json.dumps(r))
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(r, f, indent=1)
 
 
 if __name__ == "__main__":
