@@ -63,6 +63,9 @@ template <int V> struct BRow<256, V> { static constexpr int T = 32, G = 8; };
 template <int V> struct BRow<512, V> { static constexpr int T = (V == 0 ? 32 : 64), G = BT / T; };
 template <int V> struct BRow<1024, V> { static constexpr int T = (V == 0 ? 32 : 64), G = BT / T; };
 
+// The persistent kernel records no p-observables (Mp = 0), so its column
+// tiles never touch the per-bin sum buffer that follows the exchange buffer:
+// the exchange buffer alone is allocated (keeps three CTAs per SM possible).
 template <int N, int V> constexpr size_t bcol_smem() {
   return col_ex_reals<float, N, BCol<N, V>::T, BCol<N, V>::CP>() * sizeof(float);
 }

@@ -129,7 +129,7 @@ static cudaError_t launch_row_n(const PassArgs& a, cudaStream_t st) {
 
 template <typename Rl, int N, int T, int CP, int MINB>
 static cudaError_t launch_col_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
-  const size_t smem = col_ex_reals<Rl, N, T, CP>() * sizeof(Rl);
+  const size_t smem = col_smem_bytes<Rl, N, T, CP>();
   auto kern = col_pass_kernel<Rl, N, T, CP, MINB>;
   static bool attr = false;
   if (!attr) {

@@ -215,9 +215,9 @@ template <typename Rl> struct MidSums {
 //   sum_p a(p)        = A_0
 //   sum_p a(p)^2      = sum_k |A_k|^2 / N
 //   sum_p a(p) w(p)   = sum_k Re(A_k conj(Wh_k)) / N,  Wh = DFT(w)
-template <typename Rl, int N, int T, int RV, typename EX>
+template <typename Rl, int N, int T, int RV, int CP, typename EX>
 __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (&v)[RV], const int j, EX& ex,
-                                          int xa, MidSums<Rl>& o) {
+                                          int xa, int c, cplx_t<Rl>* psum, MidSums<Rl>& o) {
   using C = cplx_t<Rl>;
   const int X = a.X;
   const size_t esz = a.tab_real ? sizeof(Rl) : sizeof(C);
@@ -260,18 +260,33 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
         o.ca = A.x;
         o.cb = Bi.y;
       }
-      const Rl ur = A.x + Bi.y, ui = A.y - Bi.x;  // 2 x (spectrum a + spectrum b)
       if (a.Mp > 0) {
-        C g[MAXO];
-        load_bin_weights<Rl>(G + (size_t)k * MAXO, a.Mp, g);
+        // 2 x (spectrum a + spectrum b), summed over the tile's CP column pairs
+        // (lanes c of one row group are adjacent); one lane per bin stores it
+        Rl ur = A.x + Bi.y, ui = A.y - Bi.x;
 #pragma unroll
-        for (int q = 0; q < MAXO; ++q)
-          if (q < a.Mp) o.sq[q] += ur * g[q].x + ui * g[q].y;
+        for (int off = CP / 2; off > 0; off >>= 1) {
+          ur += __shfl_xor_sync(0xffffffffu, ur, off);
+          ui += __shfl_xor_sync(0xffffffffu, ui, off);
+        }
+        if (c == 0) psum[k] = mk<C>(ur, ui);
       }
     }
     v[m] = cscale(cadd(cmul(A, ea2), cmul(Bi, eb2)), h);
   }
   ex.sync();
+  if (obs && a.Mp > 0) {
+    // the p-weight sums: each bin's tile sum against its weight spectra, the
+    // weights loaded once per bin and CTA
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+      const C u = psum[k];
+      C g[MAXO];
+      load_bin_weights<Rl>(G + (size_t)k * MAXO, a.Mp, g);
+#pragma unroll
+      for (int q = 0; q < MAXO; ++q)
+        if (q < a.Mp) o.sq[q] += u.x * g[q].x + u.y * g[q].y;
+    }
+  }
 }
 
 // Reduce MidSums over the CTA (column-interleaved layout: lane c of a row
@@ -334,6 +349,11 @@ __device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, in
 // Reals of shared memory a column tile's exchange buffer takes: CP
 // interleaved transforms, two components, one pad slot per RV = N/T elements.
 template <typename Rl, int N, int T, int CP> constexpr size_t col_ex_reals() { return (size_t)2 * (N + T) * CP; }
+// Dynamic shared memory of a column tile: the exchange buffer, then N complex
+// per-bin sums of the tile's column spectra (p-observables of the fused pass).
+template <typename Rl, int N, int T, int CP> constexpr size_t col_smem_bytes() {
+  return (col_ex_reals<Rl, N, T, CP>() + (size_t)2 * N) * sizeof(Rl);
+}
 
 template <typename Rl, int N, int T, int CP, bool STW = false>
 __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int ntiles, unsigned char* smem_raw,
@@ -375,7 +395,8 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
   if (a.fuse_mid) {
     fft<N, T, RV, -1, C, EXT, STW>(v, j, ex, tw);
     MidSums<Rl> o;
-    fused_mid<Rl, N, T, RV>(a, b, v, j, ex, xa, o);
+    C* psum = reinterpret_cast<C*>(re + col_ex_reals<Rl, N, T, CP>());
+    fused_mid<Rl, N, T, RV, CP>(a, b, v, j, ex, xa, c, psum, o);
     if (a.part_out != nullptr) mid_store<Rl, N, CP, CP * T>(a, b, tile, ntiles, o, xa, ored);
     fft<N, T, RV, +1, C, EXT, STW>(v, j, ex, tw);
     col_store<Rl, N, T, RV>(a, v, W, j, xa);
