@@ -10,6 +10,7 @@ import os
 import re
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -73,6 +74,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     objs = []
     nvcc = _nvcc()
+    jobs = []
     for src in _sources():
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
@@ -81,7 +83,12 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
+    # the translation units are independent: compile them concurrently
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in jobs]:
+            f.result()
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart", "-lnvrtc"]
         if verbose:
