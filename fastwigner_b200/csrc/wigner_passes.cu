@@ -23,22 +23,27 @@ __global__ void __launch_bounds__(CP* T, MINB) col_pass_kernel(PassArgs a) {
   col_tile<Rl, N, T, CP>(a, blockIdx.y, blockIdx.x, gridDim.x, smem_raw, red, ored);
 }
 
-// Per-instance totals of a pass's partial-sum records: block b, thread m < M
-// sums column m of instance b's records in record order (deterministic) into
-// tot[b*M + m], and into hist[b*M + m] when hist is set.
+// Per-instance totals of a pass's partial-sum records: block b, warp m < M
+// sums column m of instance b's records (lane l takes records l, l + 32, ...,
+// then a fixed shuffle tree: deterministic) into tot[b*M + m], and into
+// hist[b*M + m] when hist is set.
 __global__ void totals_kernel(const double* part, int nparts, int M, double* tot, double* hist) {
-  const int b = blockIdx.x, m = threadIdx.x;
-  if (m >= M) return;
+  const int b = blockIdx.x, m = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (m >= M) return;  // whole warps
   const double* pp = part + (size_t)b * nparts * M + m;
   double s = 0.0;
-  for (int c = 0; c < nparts; ++c) s += pp[(size_t)c * M];
-  tot[(size_t)b * M + m] = s;
-  if (hist != nullptr) hist[(size_t)b * M + m] = s;
+  for (int c = lane; c < nparts; c += 32) s += __ldcg(pp + (size_t)c * M);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    tot[(size_t)b * M + m] = s;
+    if (hist != nullptr) hist[(size_t)b * M + m] = s;
+  }
 }
 
 cudaError_t launch_totals(const double* part, int nparts, int M, int batch, double* tot, double* hist,
                           cudaStream_t st) {
-  totals_kernel<<<batch, 32, 0, st>>>(part, nparts, M, tot, hist);
+  totals_kernel<<<batch, 32 * M, 0, st>>>(part, nparts, M, tot, hist);
   return cudaGetLastError();
 }
 
