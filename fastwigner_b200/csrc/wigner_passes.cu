@@ -70,7 +70,7 @@ template <typename Rl, int N> struct ColCfg;
 template <> struct RowCfg<float, 128> { static constexpr int T = 16, G = 16, MINB = 1; };
 template <> struct RowCfg<float, 256> { static constexpr int T = 32, G = 4, MINB = 2; };
 template <> struct RowCfg<float, 512> { static constexpr int T = 32, G = 4, MINB = 2; };
-template <> struct RowCfg<float, 1024> { static constexpr int T = 32, G = 4, MINB = 2; };
+template <> struct RowCfg<float, 1024> { static constexpr int T = 32, G = 4, MINB = 3; };
 template <> struct RowCfg<float, 2048> { static constexpr int T = 64, G = 4, MINB = 1; };
 template <> struct RowCfg<float, 4096> { static constexpr int T = 128, G = 2, MINB = 1; };
 template <> struct RowCfg<double, 128> { static constexpr int T = 16, G = 16, MINB = 1; };
