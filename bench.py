@@ -100,19 +100,46 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per grid point per column-pass launch from the committed ncu
-    summary (profiles/col_pass_f32_1024.md, line 'dram_bytes_per_point: <v>')."""
-    f = ROOT / "profiles" / "col_pass_f32_1024.md"
-    if not f.exists():
-        return None
-    for ln in f.read_text().splitlines():
-        if ln.strip().startswith("dram_bytes_per_point:"):
-            try:
-                return float(ln.split(":", 1)[1])
-            except ValueError:
-                return None
-    return None
+# DRAM bytes (read + write) per grid point of one column-pass launch, from the
+# ncu capture summarised in profiles/col_pass_f32_1024.md (dram__bytes_read.sum
+# + dram__bytes_write.sum of a 40-instance 1024 x 1024 launch / its points);
+# the line's roofline.traffic scales it to the points of one bench launch.
+NCU_COL_DRAM_BYTES_PER_POINT = 6.887
+
+
+def parity_check(sim, W0, steps=20):
+    """Outside the timed region: restart the bench plan from the initial
+    states, advance it `steps` steps and compare its first and last instance
+    with the FP64 oracle (the checker, oracle/wigner_oracle.py).  Returns
+    the largest relative L2 error of W and the largest error of an Ehrenfest
+    observable relative to that observable's largest magnitude."""
+    import torch
+
+    from oracle.wigner_oracle import WignerOracle
+
+    sim.t = 0.0
+    sim.set_wignerfunctions(W0.cuda())
+    W0n = sim.W.double().cpu().numpy()
+    obs = sim.propagate(steps).cpu().numpy()
+    torch.cuda.synchronize()
+    W = sim.W.double().cpu().numpy()
+    rel_l2, obs_rel = 0.0, 0.0
+    insts = sorted({0, sim.batch - 1})
+    for b in insts:
+        o = WignerOracle(X_gridDIM=GRID, X_amplitude=AMP, P_gridDIM=GRID, P_amplitude=AMP, dt=DT, V=V, K=K,
+                         diff_V=dV, diff_K=dK, fft_workers=os.cpu_count())
+        o.cache_exponents()
+        o.set_wignerfunction(W0n[b])
+        o.propagate(steps)
+        rel_l2 = max(rel_l2, float(np.linalg.norm(W[b] - o.W) / np.linalg.norm(o.W)))
+        s = obs[:, b, 0]
+        got = {"X_average": obs[:, b, 2] / s, "P_average_RHS": -obs[:, b, 3] / s, "P_average": obs[:, b, 5] / s,
+               "X_average_RHS": obs[:, b, 6] / s, "hamiltonian_average": (obs[:, b, 4] + obs[:, b, 7]) / s}
+        for k, g in got.items():
+            r = np.asarray(getattr(o, k))
+            obs_rel = max(obs_rel, float(np.abs(g - r).max() / np.abs(r).max()))
+    return {"rel_l2": rel_l2, "max_obs_rel": obs_rel, "steps": steps, "instances": insts,
+            "against": "FP64 oracle (numpy restatement of WignerMoyalFTTW1D.propagate)", "tol_rel_l2": 1e-5}
 
 
 # ---------------------------------------------------------------------------
@@ -140,6 +167,9 @@ def cpu_reference_rate(target_s, steps=None, grid=GRID, workers=None):
     return grid * grid * steps / el, steps, el, cores
 
 
+REF_SAMPLE_INSTANCES = 8  # instances of the batch the reference arm advances per bench step
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -147,24 +177,36 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     from oracle.wigner_oracle import WignerOracle
 
-    o = WignerOracle(X_gridDIM=GRID, X_amplitude=AMP, P_gridDIM=GRID, P_amplitude=AMP, dt=DT,
-                     V=V, K=K, diff_V=dV, diff_K=dK, fft_workers=cores)
-    o.cache_exponents()
+    n = min(REF_SAMPLE_INSTANCES, args.batch)
     rng = np.random.default_rng(12345)
-    o.set_wignerfunction(initial_states(rng, 1, o.X, o.P)[0].astype(np.float64))
-    o.propagate(args.warmup)
+    inst = []
+    for _ in range(n):
+        o = WignerOracle(X_gridDIM=GRID, X_amplitude=AMP, P_gridDIM=GRID, P_amplitude=AMP, dt=DT,
+                         V=V, K=K, diff_V=dV, diff_K=dK, fft_workers=cores)
+        o.cache_exponents()
+        o.set_wignerfunction(initial_states(rng, 1, o.X, o.P)[0].astype(np.float64))
+        inst.append(o)
+
+    def step():  # one time step of the sampled instances
+        for o in inst:
+            o.propagate(1)
+
+    for _ in range(args.warmup):
+        step()
     t0 = time.perf_counter()
-    o.propagate(args.steps)
+    for _ in range(args.steps):
+        step()
     el = time.perf_counter() - t0
-    value = GRID * GRID * args.steps / el
-    sample = f"1 instance of the {GRID}x{GRID} workload, {args.steps} FP64 steps, scipy.fft workers={cores}"
+    value = GRID * GRID * n * args.steps / el
+    sample = (f"{n} instances of the {GRID}x{GRID} workload per step, {args.steps} FP64 steps, "
+              f"scipy.fft workers={cores}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"moyal_double_well_{GRID}x{GRID}_batch{args.batch}", "grid": [GRID, GRID],
                    "batch_per_gpu": args.batch, "dt": DT, "potential": "0.05 x^4 - x^2", "amplitudes": [AMP, AMP],
-                   "sample": f"one of the {args.batch} instances per step (the metric is per grid point)",
+                   "sample": f"{n} of the {args.batch} instances per step (the metric is per grid point)",
                    "implementation": "FP64 numpy restatement of WignerMoyalFTTW1D"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -239,9 +281,10 @@ def run_ours(args):
     peak, peak_kind = measured_peak_gbs()
     alg_bytes = BYTES_PER_PT_PASS * pts
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
-    tpp = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": (tpp * pts) if tpp is not None else None,
+                "traffic": NCU_COL_DRAM_BYTES_PER_POINT * pts,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per point of a column-pass "
+                                  "launch (profiles/col_pass_f32_1024.md), times the points of one launch",
                 "kernel": dom_kind, "kernel_ms": dom_ms, "col_ms": col_ms, "row_ms": row_ms,
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
                 "frac_of_nominal_8000_gbs": achieved / 8000.0}
@@ -273,6 +316,8 @@ def run_ours(args):
     h2d = W0_pinned.numel() * 4 / E2E_STEPS
     d2h = (host_out[0].numel() * 4 + obs_host[0].numel() * 8) / E2E_STEPS
 
+    parity = parity_check(sim, W0_pinned) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, csteps, cel, cores = cpu_reference_rate(args.cpu_seconds)
@@ -297,6 +342,7 @@ def run_ours(args):
                                    f"back to pinned host (copies overlap the neighbouring batches)",
                        "e2e_finite": e2e_finite},
             "roofline": roofline,
+            "parity": parity,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

@@ -74,6 +74,7 @@ _SIGNATURES = [
     ("fw_launch_count", c_ll, []),
     ("fw_wigner_propagate_noalloc", c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(WignerDesc), c_int, c_vp]),
     ("fw_noalloc_scratch_bytes", ctypes.c_size_t, []),
+    ("fw_noalloc_scratch_needed", ctypes.c_size_t, [c_int, c_int, c_int, c_int, ctypes.POINTER(WignerDesc)]),
     ("fw_rho_plan_create", c_int, [c_int, c_int, c_int, ctypes.POINTER(c_vp)]),
     ("fw_rho_plan_destroy", c_int, [c_vp]),
     ("fw_rho_num_parts", c_int, [c_vp]),
@@ -87,6 +88,8 @@ _SIGNATURES = [
     ("fw_batch_set_instance", c_int, [c_vp, c_int, c_vp, c_vp, c_vp, c_dbl]),
     ("fw_batch_propagate", c_int, [c_vp, c_int, c_vp, c_int, c_vp]),
     ("fw_batch_status", c_int, [c_vp, ctypes.POINTER(c_int)]),
+    ("fw_batch_set_status", c_int, [c_vp, c_int]),
+    ("fw_batch_set_spin_limit", c_int, [c_vp, c_ll]),
     ("fw_fno_sgemm", c_int, [c_int, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_ll, c_ll, c_vp, c_ll, c_ll,
                               ctypes.c_float, c_vp, c_ll, c_ll, c_int, c_vp]),
     ("fw_fno_mix", c_int, [c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),

@@ -291,6 +291,16 @@ class WignerMoyalUnevenBatch:
         check(self._lib.fw_batch_status(self._h, ctypes.byref(st)), "fw_batch_status")
         return st.value
 
+    def set_status(self, value=0):
+        """Write the device status word: 0 clears a recorded FW_BATCH_TIMEOUT;
+        a non-zero value makes the next launch return at its first grid barrier."""
+        check(self._lib.fw_batch_set_status(self._h, int(value)), "fw_batch_set_status")
+
+    def set_spin_limit(self, polls):
+        """Polls a CTA waits at a grid barrier before the launch gives up with
+        FW_BATCH_TIMEOUT (default 2**25, a few seconds)."""
+        check(self._lib.fw_batch_set_spin_limit(self._h, int(polls)), "fw_batch_set_spin_limit")
+
     def purity(self, obs):
         """2 pi hbar sum(W^2) dXdP of the normalised states, from propagate()'s sums."""
         o = obs.cpu().numpy() if isinstance(obs, torch.Tensor) else obs

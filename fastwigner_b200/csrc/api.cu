@@ -430,13 +430,15 @@ extern "C" int fw_wigner_weighted_sum(fw_wigner_plan* plan, const void* W, long 
 // loop that must not hit the implicit device-wide synchronisation of
 // cudaMalloc / cudaFree between propagation calls.  For them,
 // fw_wigner_propagate_noalloc runs the same passes as fw_wigner_propagate
-// with the plan scratch (twiddle tables and the partial-sum ring) placed in
-// the fixed array below instead of plan allocations.
+// with the plan scratch (twiddle tables, the partial-sum ring, the
+// per-instance totals and the p-weight spectra) placed in the fixed array
+// below instead of plan allocations.
 namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB per device, held until process exit
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
-constexpr int kMaxDevices = 64;
+// device address of g_noalloc_scratch per device, looked up once per device
 static unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+static PerDeviceOnce g_noalloc_once;
 
 __global__ void noalloc_twiddles_kernel(int n, int dtype, void* out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -472,64 +474,99 @@ __global__ void noalloc_stage_kernel(int n, int rv, int dtype, const void* tw, v
 }
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
-}  // namespace
 
-extern "C" size_t fw_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+// Byte offsets of the no-allocation scratch regions of one call, in the
+// order they sit in the array, each starting on 256 bytes.
+struct NoAllocLayout {
+  int small, np, rvX, nsX, wph_nb;
+  size_t twP, twX, twsX, ring, tot, wph, need;
+};
 
-extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, const fw_wigner_desc* desc, int steps,
-                                           void* stream) {
-  if (desc == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: NULL desc");
+// Layout for a call with these sizes and descriptor; returns FW_OK or an
+// FW_EINVAL message (sizes the plan entry point would also reject).
+int noalloc_layout(int P, int X, int batch, int dtype, const fw_wigner_desc* d, NoAllocLayout* L) {
   if (dtype != FW_F32 && dtype != FW_F64) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: bad dtype");
   if (!size_supported(P) || !size_supported(X))
     return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: P and X must be powers of two in [128, 4096]");
   if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: batch must be in [1, 65535]");
-  const int small = small_shapes(dtype, P, X, batch);
-  const int np = col_parts(dtype, P, X, small);
-  if (np <= 0) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: unsupported X for the column pass tile");
+  L->small = small_shapes(dtype, P, X, batch);
+  L->np = col_parts(dtype, P, X, L->small);
+  if (L->np <= 0) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: unsupported X for the column pass tile");
   const size_t rs = dtype == FW_F64 ? sizeof(double) : sizeof(float);
-  const size_t twP_bytes = align256(2 * rs * (size_t)P);
-  const size_t twX_bytes = align256(2 * rs * (size_t)X);
-  const int rvX = row_rv(dtype, X, small);
-  const int nsX = stage_off(X, rvX, X);
-  const size_t twsX_bytes = align256(2 * rs * (size_t)(nsX > 0 ? nsX : 1));
-  const size_t ring_bytes = sizeof(double) * 2 * (size_t)batch * np * MMAX;
-  const size_t need = twP_bytes + twX_bytes + twsX_bytes + ring_bytes;
-  if (need > kNoAllocScratchBytes)
-    return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: needs " + std::to_string(need) +
+  L->rvX = row_rv(dtype, X, L->small);
+  L->nsX = stage_off(X, L->rvX, X);
+  // p-weight spectra (fused mid-point column pass): shared or per-instance weights
+  const bool pw = d != nullptr && d->Mp > 0;
+  L->wph_nb = pw ? (d->wp_bstride != 0 ? batch : 1) : 0;
+  size_t off = 0;
+  L->twP = off;  off += align256(2 * rs * (size_t)P);
+  L->twX = off;  off += align256(2 * rs * (size_t)X);
+  L->twsX = off; off += align256(2 * rs * (size_t)(L->nsX > 0 ? L->nsX : 1));
+  L->ring = off; off += align256(sizeof(double) * 2 * (size_t)batch * L->np * MMAX);
+  L->tot = off;  off += align256(sizeof(double) * (size_t)batch * MMAX);
+  L->wph = off;  off += align256((size_t)4 * P * 2 * rs * (size_t)L->wph_nb);
+  L->need = off;
+  return FW_OK;
+}
+}  // namespace
+
+extern "C" size_t fw_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" size_t fw_noalloc_scratch_needed(int P, int X, int batch, int dtype, const fw_wigner_desc* desc) {
+  NoAllocLayout L;
+  return noalloc_layout(P, X, batch, dtype, desc, &L) == FW_OK ? L.need : 0;
+}
+
+extern "C" int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, const fw_wigner_desc* desc, int steps,
+                                           void* stream) {
+  if (desc == nullptr) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: NULL desc");
+  NoAllocLayout L;
+  int rc = noalloc_layout(P, X, batch, dtype, desc, &L);
+  if (rc != FW_OK) return rc;
+  if (L.need > kNoAllocScratchBytes)
+    return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: needs " + std::to_string(L.need) +
                                " bytes of scratch for this grid and batch, more than the fixed " +
                                std::to_string(kNoAllocScratchBytes) + " bytes; use fw_wigner_propagate");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: device index too large");
-  if (g_noalloc_ptr[dev] == nullptr) {  // once per device, with that device current
+  // once per device, with that device current (thread-safe)
+  e = g_noalloc_once.run([&] {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
-    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
-  }
+    cudaError_t r = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (r == cudaSuccess) g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    return r;
+  });
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
   unsigned char* base = g_noalloc_ptr[dev];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // every call rewrites the twiddles (earlier calls may have left other sizes);
-  // the partial-sum ring is always written before it is read
-  noalloc_twiddles_kernel<<<(P + 255) / 256, 256, 0, st>>>(P, dtype, base);
-  noalloc_twiddles_kernel<<<(X + 255) / 256, 256, 0, st>>>(X, dtype, base + twP_bytes);
-  unsigned char* twsX = base + twP_bytes + twX_bytes;
-  if (nsX > 0) noalloc_stage_kernel<<<(nsX + 255) / 256, 256, 0, st>>>(X, rvX, dtype, base + twP_bytes, twsX, nsX);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "noalloc twiddle launch");
-  count_launch(2 + (nsX > 0));
+  if (steps > 0) {
+    // every call rewrites the twiddles (earlier calls may have left other
+    // sizes); the partial-sum ring, the totals and the weight spectra are
+    // always written before they are read
+    noalloc_twiddles_kernel<<<(P + 255) / 256, 256, 0, st>>>(P, dtype, base + L.twP);
+    noalloc_twiddles_kernel<<<(X + 255) / 256, 256, 0, st>>>(X, dtype, base + L.twX);
+    if (L.nsX > 0)
+      noalloc_stage_kernel<<<(L.nsX + 255) / 256, 256, 0, st>>>(X, L.rvX, dtype, base + L.twX, base + L.twsX, L.nsX);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "noalloc twiddle launch");
+    count_launch(2 + (L.nsX > 0));
+  }
   fw_wigner_plan tmp;
   tmp.P = P;
   tmp.X = X;
   tmp.batch = batch;
   tmp.dtype = dtype;
-  tmp.nparts = np;
-  tmp.small = small;
-  tmp.twP = base;
-  tmp.twX = base + twP_bytes;
-  tmp.twsX = twsX;
-  tmp.ring = reinterpret_cast<double*>(twsX + twsX_bytes);
+  tmp.nparts = L.np;
+  tmp.small = L.small;
+  tmp.twP = base + L.twP;
+  tmp.twX = base + L.twX;
+  tmp.twsX = base + L.twsX;
+  tmp.ring = reinterpret_cast<double*>(base + L.ring);
+  tmp.tot = reinterpret_cast<double*>(base + L.tot);
+  tmp.wph = L.wph_nb > 0 ? base + L.wph : nullptr;
+  tmp.wph_nb = L.wph_nb;
   tmp.wsum = nullptr;
   tmp.wsum_blocks = 0;
   return fw_wigner_propagate(&tmp, desc, steps, stream);

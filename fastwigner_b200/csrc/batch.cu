@@ -246,6 +246,7 @@ struct fw_batch {
   int counters_cap = 0;
   unsigned int* barrier = nullptr;
   int* status = nullptr;
+  long long spin_limit = 1LL << 25;  // polls per barrier wait (~2-4 s) before the launch gives up
   int grid = 0;
   bool dirty = true;
   // CUDA graph of the last propagate(steps, obs)
@@ -388,7 +389,7 @@ int launch(fw_batch* b, int steps, double* obs, cudaStream_t st) {
   a.counters = b->counters;
   a.barrier = b->barrier;
   a.status = b->status;
-  a.spin_limit = 1LL << 25;  // ~2-4 s of polling per barrier before the launch gives up
+  a.spin_limit = b->spin_limit;
   void* args[] = {&a};
   const void* kp = b->variant ? kernel_ptr<1>() : kernel_ptr<0>();
   const size_t smem = b->variant ? kernel_smem<1>() : kernel_smem<0>();
@@ -497,6 +498,22 @@ extern "C" int fw_batch_status(fw_batch* b, int* status_out) {
   if (b == nullptr || status_out == nullptr) return fail(FW_EINVAL, "fw_batch_status: NULL argument");
   cudaError_t e = cudaMemcpy(status_out, b->status, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "fw_batch_status");
+  return FW_OK;
+}
+
+extern "C" int fw_batch_set_spin_limit(fw_batch* b, long long polls) {
+  if (b == nullptr || polls < 0) return fail(FW_EINVAL, "fw_batch_set_spin_limit: bad arguments");
+  if (b->spin_limit != polls) {
+    b->spin_limit = polls;
+    release_graph(b);  // a captured launch holds the old limit in its arguments
+  }
+  return FW_OK;
+}
+
+extern "C" int fw_batch_set_status(fw_batch* b, int status) {
+  if (b == nullptr) return fail(FW_EINVAL, "fw_batch_set_status: NULL batch");
+  cudaError_t e = cudaMemcpy(b->status, &status, sizeof(int), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "fw_batch_set_status");
   return FW_OK;
 }
 

@@ -1,10 +1,36 @@
 // Internal declarations shared by the CUDA translation units of libfastwigner.
 #pragma once
 #include <cuda_runtime.h>
+#include <mutex>
 #include <string>
 #include "../../include/fastwigner.h"
 
 namespace fw {
+constexpr int kMaxDevices = 64;
+
+// A set-up call made once per device and remembered (thread-safe): e.g. the
+// dynamic shared-memory limit of one kernel, which is a per-device attribute.
+// The first call on a device runs `fn` with that device current; later calls
+// on it return the recorded result.  cudaDeviceReset does not clear the record.
+struct PerDeviceOnce {
+  std::once_flag flag[kMaxDevices];
+  cudaError_t err[kMaxDevices] = {};
+  template <class Fn> cudaError_t run(Fn&& fn) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::call_once(flag[dev], [&] { err[dev] = fn(); });
+    return err[dev];
+  }
+};
+
+// Raise a kernel's dynamic shared-memory limit to `smem` bytes, once per
+// device and kernel (each call site keeps its own PerDeviceOnce).
+template <typename K> cudaError_t set_smem_once(PerDeviceOnce& once, K kern, size_t smem) {
+  return once.run([&] { return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); });
+}
+
 struct PassArgs;
 cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st);
 cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* nparts);

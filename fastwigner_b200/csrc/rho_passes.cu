@@ -351,12 +351,9 @@ static cudaError_t rho_row_sh(const RhoArgs& a, cudaStream_t st, int* nparts) {
   constexpr int T = Cfg::T, G = Cfg::G, MINB = Cfg::MINB;
   const size_t smem = (size_t)G * 2 * (N + N / 32) * sizeof(Rl);
   auto kern = rho_row_kernel<Rl, N, T, G, MINB, SH>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per device: the attribute is set on the device current at the call
+  cudaError_t e = set_smem_once(attr, kern, smem);
+  if (e != cudaSuccess) return e;
   dim3 grid(N / G, a.batch);
   if (nparts) *nparts = grid.x;
   kern<<<grid, G * T, smem, st>>>(a);
@@ -377,12 +374,9 @@ static cudaError_t rho_col_sh(const RhoArgs& a, cudaStream_t st) {
   constexpr int S = ilog2_c(N / T > 32 ? 32 : N / T);
   const size_t smem = (size_t)2 * N * CP * sizeof(Rl);
   auto kern = rho_col_kernel<Rl, N, T, CP, S, MINB, SH>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per device: the attribute is set on the device current at the call
+  cudaError_t e = set_smem_once(attr, kern, smem);
+  if (e != cudaSuccess) return e;
   dim3 grid(N / CP, a.batch);
   kern<<<grid, CP * T, smem, st>>>(a);
   return cudaGetLastError();

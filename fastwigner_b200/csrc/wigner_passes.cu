@@ -111,12 +111,9 @@ template <typename Rl, int N, int T, int G, int MINB>
 static cudaError_t launch_row_cfg(const PassArgs& a, cudaStream_t st) {
   const size_t smem = (size_t)G * 2 * (N + N / 32) * sizeof(Rl);
   auto kern = row_pass_kernel<Rl, N, T, G, MINB>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per device: the attribute is set on the device current at the call
+  cudaError_t e = set_smem_once(attr, kern, smem);
+  if (e != cudaSuccess) return e;
   dim3 grid((a.P / 2 + G - 1) / G, a.batch);
   kern<<<grid, G * T, smem, st>>>(a);
   return cudaGetLastError();
@@ -136,12 +133,9 @@ template <typename Rl, int N, int T, int CP, int MINB>
 static cudaError_t launch_col_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
   const size_t smem = col_smem_bytes<Rl, N, T, CP>();
   auto kern = col_pass_kernel<Rl, N, T, CP, MINB>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per device: the attribute is set on the device current at the call
+  cudaError_t e = set_smem_once(attr, kern, smem);
+  if (e != cudaSuccess) return e;
   dim3 grid(a.X / (2 * CP), a.batch);
   if (nparts) *nparts = grid.x;
   kern<<<grid, CP * T, smem, st>>>(a);

@@ -200,11 +200,14 @@ __device__ __forceinline__ void col_store(const PassArgs& a, const cplx_t<Rl> (&
   }
 }
 
-// Per-thread partial sums of a fused column pass, in the state precision:
-// sum |2A_k|^2 + |2B_k|^2 over the thread's bins, sum Re(2(A_k+B_k) conj(Wh_k))
-// per p-weight, and (thread j == 0 only) the doubled DC bins of the pair.
+// Per-thread partial sums of a fused column pass, accumulated in FP64 whatever
+// the state precision: sum |2A_k|^2 + |2B_k|^2 over the thread's bins (each
+// bin's four squares summed in the state precision -- positive terms, so
+// that short sum has no cancellation -- then added in FP64), sum
+// Re(2(A_k+B_k) conj(Wh_k)) per p-weight, and (thread j == 0 only) the
+// doubled DC bins of the pair.
 template <typename Rl> struct MidSums {
-  Rl s2, sq[MAXO], ca, cb;
+  double s2, sq[MAXO], ca, cb;
 };
 
 // Mid-point of a fused column pass (a.fuse_mid): v holds the forward spectrum
@@ -255,7 +258,7 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
     const C A = cmul(cadd(v[m], zc), ea1);   // 2 x spectrum of column a at the mid-point
     const C Bi = cmul(csub(v[m], zc), eb1);  // 2i x spectrum of column b at the mid-point
     if (obs) {
-      o.s2 += A.x * A.x + A.y * A.y + Bi.x * Bi.x + Bi.y * Bi.y;
+      o.s2 += (double)(A.x * A.x + A.y * A.y + Bi.x * Bi.x + Bi.y * Bi.y);
       if (m == 0 && j == 0) {  // DC bin: the column sums
         o.ca = A.x;
         o.cb = Bi.y;
@@ -284,15 +287,15 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
       load_bin_weights<Rl>(G + (size_t)k * MAXO, a.Mp, g);
 #pragma unroll
       for (int q = 0; q < MAXO; ++q)
-        if (q < a.Mp) o.sq[q] += u.x * g[q].x + u.y * g[q].y;
+        if (q < a.Mp) o.sq[q] += (double)u.x * (double)g[q].x + (double)u.y * (double)g[q].y;
     }
   }
 }
 
 // Reduce MidSums over the CTA (column-interleaved layout: lane c of a row
 // group is column pair c) and write the tile's partial-sum record.  The bin
-// sums reduce in the state precision within each warp, then in FP64 across
-// warps; the DC terms live in threads j == 0 (tid < CP, all in warp 0).
+// sums reduce in FP64 within each warp (shuffle tree) and across warps; the
+// DC terms live in threads j == 0 (tid < CP, all in warp 0).
 template <typename Rl, int N, int CP, int NTHR>
 __device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, int ntiles, MidSums<Rl>& o, int xa,
                                           double (*ored)[2 + 2 * MAXO]) {
@@ -306,12 +309,12 @@ __device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, in
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0) {
-    ored[warp][1] = (double)o.s2 * (0.25 / (double)N);
+    ored[warp][1] = o.s2 * (0.25 / (double)N);
 #pragma unroll
-    for (int q = 0; q < MAXO; ++q) ored[warp][2 + MAXO + q] = (double)o.sq[q] * (0.5 / (double)N);
+    for (int q = 0; q < MAXO; ++q) ored[warp][2 + MAXO + q] = o.sq[q] * (0.5 / (double)N);
   }
   if (warp == 0) {
-    const double da = 0.5 * (double)o.ca, db = 0.5 * (double)o.cb;
+    const double da = 0.5 * o.ca, db = 0.5 * o.cb;
     double d[1 + MAXO];
     d[0] = da + db;
     const double* wx = a.wx + (size_t)b * a.wx_bs;
@@ -438,9 +441,10 @@ __device__ __forceinline__ void col_tile(const PassArgs& a, int b, int tile, int
     const int P = N;
     if constexpr (sizeof(Rl) == 4) {
       // FP32 state: the 2*CP columns of a row sit in CP adjacent lanes; reduce a
-      // row's sums across them with shuffles, then one lane per row accumulates
-      // the FP64 weighted sums (per-thread column sums over RV rows in FP32).
-      float fa = 0.f, fb = 0.f;
+      // row's sums across them with shuffles (log2 CP additions), then one lane
+      // per row accumulates the FP64 weighted sums; the per-thread column sums
+      // over RV rows accumulate in FP64.
+      double fa = 0.0, fb = 0.0;
       constexpr int CH = RV < 8 ? RV : 8;  // rows per batch of independent shuffles
 #pragma unroll
       for (int m0 = 0; m0 < RV; m0 += CH) {

@@ -363,8 +363,12 @@ class _WignerBase:
         return 1.0
 
     def get_purity(self):
-        """2 pi hbar sum(W^2) dX dP."""
-        return 2.0 * np.pi * self.hbar * float((self._W.double() ** 2).sum()) * self.dXdP
+        """2 pi hbar sum(W^2) dX dP (wigner_moyal_cuda_1d.py:398-403), the sum
+        of squares reduced in FP64 on the device by fw_wigner_weighted_sum."""
+        out = torch.empty(2, dtype=torch.float64, device=self.device)
+        check(self._lib.fw_wigner_weighted_sum(self._plan, ptr(self._W), self._W.numel(), None, ptr(out),
+                                               stream_handle()), "fw_wigner_weighted_sum")
+        return 2.0 * np.pi * self.hbar * float(out[1]) * self.dXdP
 
     def _grid_average(self, F):
         """sum(W * F) dXdP with F a P x X FP64 grid, reduced on the device."""

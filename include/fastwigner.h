@@ -149,21 +149,35 @@ long long fw_launch_count(void);
  * (instrument or real-time control loops that size all GPU memory at start-up),
  * or a loop that must not hit the device-wide synchronisation of cudaMalloc /
  * cudaFree between calls.  This entry point takes no plan and allocates
- * nothing: its scratch (twiddle tables and partial sums) lives in a fixed
- * array of fw_noalloc_scratch_bytes() (4 MiB) that every GPU loading the
- * library holds until exit.  Grids and batches needing more scratch
- * (2*(P+X) reals + 2*batch*(X/(2*CP))*10 doubles) are rejected with
- * FW_EINVAL.  The first call on a device looks up the array's device address
- * (make that first call before any stream capture).  All calls share the
- * array: calls that overlap on the GPU (other streams, other host threads)
- * race and must be serialised by the caller.  The caller still owns W, the
- * tables, weights and obs_out exactly as for fw_wigner_propagate.
+ * nothing: its scratch (twiddle tables, partial sums, per-instance totals and
+ * the spectra of the p-observable weights) lives in a fixed array of
+ * fw_noalloc_scratch_bytes() (4 MiB) that every GPU loading the library holds
+ * until exit, and it runs the same passes as fw_wigner_propagate with a plan
+ * of the same sizes.  A call whose scratch (fw_noalloc_scratch_needed) exceeds
+ * the array is rejected with FW_EINVAL.  The first call on a device looks up
+ * the array's device address (thread-safe, once per device; make that first
+ * call before any stream capture; after cudaDeviceReset the recorded address
+ * is stale, so a process that resets a device must not call this entry point
+ * on it again).  All calls share the array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the
+ * caller.  The caller still owns W, the tables, weights and obs_out exactly
+ * as for fw_wigner_propagate.
  */
 int fw_wigner_propagate_noalloc(int P, int X, int batch, int dtype, const fw_wigner_desc* desc, int steps,
                                 void* stream);
 
 /* Size in bytes of the fixed scratch array used by fw_wigner_propagate_noalloc. */
 size_t fw_noalloc_scratch_bytes(void);
+
+/*
+ * Bytes of that array a fw_wigner_propagate_noalloc call with these sizes and
+ * descriptor needs (only desc->Mp and desc->wp_bstride matter; desc may be
+ * NULL for no p-observables): the twiddle tables of P and X, the row pass's
+ * stage-layout table, 2 x batch x (column tiles per instance) x 10 partial
+ * sums, batch x 10 totals and, with p-observables, 4 x P weight spectra per
+ * weight set, each region rounded up to 256 bytes.  0 for invalid sizes.
+ */
+size_t fw_noalloc_scratch_needed(int P, int X, int batch, int dtype, const fw_wigner_desc* desc);
 
 /*
  * out[b*2+0] = sum_{p,x} W[b] * F (F = NULL means F = 1), out[b*2+1] = sum W^2, in FP64.
@@ -289,6 +303,22 @@ int fw_batch_set_instance(fw_batch* batch, int i, void* W, const void* tabV, con
 int fw_batch_propagate(fw_batch* batch, int steps, double* obs, int use_graph, void* stream);
 /* Synchronous read of the device status word (0 or FW_BATCH_TIMEOUT). */
 int fw_batch_status(fw_batch* batch, int* status_out);
+/*
+ * Synchronous write of the device status word.  0 clears a recorded timeout
+ * so that the batch can run again; a non-zero value makes the next launch
+ * return at its first grid barrier (every CTA reads the word there).  The
+ * status word is this build's failure detection for the persistent launch;
+ * the reference has no counterpart (its only recovery is the Bloch roll-back,
+ * wigner_bloch_cuda_1d.py:188-225).
+ */
+int fw_batch_set_status(fw_batch* batch, int status);
+/*
+ * Polls (each followed by a 64 ns sleep) that a CTA waits at a grid barrier
+ * before it records FW_BATCH_TIMEOUT and the launch returns; default 2^25
+ * (a few seconds).  0 makes any CTA that has to wait give up at once.
+ * Changing the limit drops a captured graph of the launch.
+ */
+int fw_batch_set_spin_limit(fw_batch* batch, long long polls);
 
 /* ------------------------------------------------------------------------ */
 /* Fourier-neural-operator surrogate kernels (training and inference, FP32)  */

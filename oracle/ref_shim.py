@@ -29,13 +29,15 @@ from __future__ import annotations
 
 import builtins
 import importlib.util
+import os
 import sys
 import types
 from pathlib import Path
 
 import numpy as np
 
-REFERENCE = Path("/root/reference")
+# the reference checkout; FASTWIGNER_REFERENCE overrides the default location
+REFERENCE = Path(os.environ.get("FASTWIGNER_REFERENCE", "/root/reference"))
 
 
 class _FFTWPlan:

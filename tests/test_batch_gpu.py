@@ -129,3 +129,78 @@ def test_host_batches_pipeline_equals_sequential_calls():
         np.testing.assert_array_equal(out[i].numpy(), b.W.cpu().numpy())
         np.testing.assert_array_equal(obs_out[i].numpy(), ob.cpu().numpy())
     np.testing.assert_array_equal(a.W.cpu().numpy(), out[-1].numpy())
+
+
+FW_BATCH_TIMEOUT = 1
+
+
+def _oracle_states(b, states, steps):
+    out = []
+    for s, W0 in zip(b.specs, states):
+        o = WignerOracle(X_gridDIM=s["X_gridDIM"], X_amplitude=s["X_amplitude"], P_gridDIM=s["P_gridDIM"],
+                         P_amplitude=s["P_amplitude"], dt=0.005, V=s["V"], K=s["K"])
+        o.set_wignerfunction(W0.astype(np.float64))
+        o.propagate(steps)
+        out.append(o.W)
+    return out
+
+
+def test_planted_status_makes_the_launch_return_early_and_clears():
+    """A non-zero status word planted from the host before the launch: every
+    CTA reads it at the first grid barrier and returns, the word still reads
+    FW_BATCH_TIMEOUT afterwards, and once it is cleared the same batch runs
+    normally (the context stays usable).  No wait is left unbounded."""
+    import torch
+
+    from fastwigner_b200.batch import WignerMoyalUnevenBatch
+
+    rng = np.random.default_rng(8)
+    b = WignerMoyalUnevenBatch(make_specs(rng), dt=0.005, variant=0)
+    states = [initial(s, rng) for s in b.specs]
+    b.set_wignerfunctions(states)
+    b.set_status(FW_BATCH_TIMEOUT)
+    b.propagate(2, use_graph=False)
+    torch.cuda.synchronize()
+    assert b.status() == FW_BATCH_TIMEOUT
+    b.set_status(0)
+    b.set_wignerfunctions(states)
+    b.t = 0.0
+    b.propagate(2, use_graph=False)
+    torch.cuda.synchronize()
+    assert b.status() == 0
+    for W, ref in zip(b.W, _oracle_states(b, states, 2)):
+        assert rel(W.double().cpu().numpy(), ref) < 1e-5
+
+
+def test_barrier_wait_limit_expires_and_returns():
+    """A spin limit of 0 polls: the first CTA that has to wait at a grid
+    barrier gives up at once and records FW_BATCH_TIMEOUT, the others see the
+    word and return, and the launch ends.  Afterwards (limit restored, word
+    cleared) the batch propagates correctly."""
+    import torch
+
+    from fastwigner_b200.batch import WignerMoyalUnevenBatch
+
+    rng = np.random.default_rng(9)
+    b = WignerMoyalUnevenBatch(make_specs(rng), dt=0.005, variant=0)
+    states = [initial(s, rng) for s in b.specs]
+    b.set_spin_limit(0)
+    seen = 0
+    for _ in range(3):  # the first arriver could in principle find the barrier already released
+        b.set_status(0)
+        b.set_wignerfunctions(states)
+        b.propagate(2, use_graph=False)
+        torch.cuda.synchronize()
+        seen = b.status()
+        if seen == FW_BATCH_TIMEOUT:
+            break
+    assert seen == FW_BATCH_TIMEOUT
+    b.set_spin_limit(1 << 25)
+    b.set_status(0)
+    b.set_wignerfunctions(states)
+    b.t = 0.0
+    b.propagate(2, use_graph=True)
+    torch.cuda.synchronize()
+    assert b.status() == 0
+    for W, ref in zip(b.W, _oracle_states(b, states, 2)):
+        assert rel(W.double().cpu().numpy(), ref) < 1e-5

@@ -1,14 +1,9 @@
 """GPU parity of the Wigner-function drop-ins against the reference fixtures
 and the FP64 oracle.
 
-Tolerances: FP64 runs 1e-10 relative (L2 of W and every observable).
-FP32 runs (complex64 spectra, FP64-built phases): 1e-5 relative L2 of W;
-per observable (rtol, atol) from FP32_OBS_TOL, about 3x the error of an exact
-complex64 numpy pipeline (W rounded to float32 after every pass) on the same
-cases.  Observables whose weight grows in the far tails (<V'> ~ x^3, <H>)
-inherit the FP32 round-off floor of W there multiplied by the weight
-(V(+-10) = 400 for the double well): the exact FP32 pipeline is already at
-4e-5 on -<V'> and 1.1e-4 on <H> for that case."""
+Tolerances (tests/parity_tables.py): FP64 runs 1e-10 relative (L2 of W and
+every observable); FP32 runs (complex64 spectra, FP64-built phases) 1e-5
+relative L2 of W and FP32_OBS_TOL per observable."""
 import sys
 from pathlib import Path
 
@@ -21,18 +16,12 @@ from cases import CASES, CONFIG1  # noqa: E402
 
 from oracle.wigner_oracle import WignerOracle, exact_harmonic_gibbs  # noqa: E402
 
+sys.path.insert(0, str(ROOT / "tests"))
+from parity_tables import FP32_OBS_TOL, FP32_TOL, FP64_TOL  # noqa: E402
+
 pytestmark = pytest.mark.gpu
 GOLD = ROOT / "tests" / "golden"
 OBS = ("X_average", "P_average", "X_average_RHS", "P_average_RHS", "hamiltonian_average")
-FP64_TOL = 1e-10
-FP32_TOL = 1e-5
-FP32_OBS_TOL = {
-    "X_average": (1e-5, 2e-5),
-    "P_average": (1e-5, 2e-5),
-    "X_average_RHS": (1e-5, 2e-5),
-    "P_average_RHS": (1e-4, 1.2e-4),
-    "hamiltonian_average": (5e-4, 3e-4),
-}
 
 
 def fw():
