@@ -176,6 +176,28 @@ class RhoOracle:
         self.rho /= np.trace(self.rho) * self.dX
         return self.rho
 
+    def get_ground_state(self, dbeta, abs_tol_purity=1e-12):
+        """rho_bloch_cuda_1d.py:162-221: imaginary-time steps from the delta
+        state, each accepted only if the purity stays <= 1 and the energy
+        Tr[rho K] + Tr[rho V] decreased; otherwise the previous state is
+        restored and dbeta halved."""
+        prev_e = cur_e = np.inf
+        prev_p = cur_p = 0.0
+        self.set_rho(np.eye(self.N))
+        prev = self.rho.copy()
+        while cur_p < (1.0 - abs_tol_purity) and dbeta > 1e-12:
+            self.bloch_single_step(dbeta)
+            cur_p = self.get_purity()
+            cur_e = self.get_average((None, self._k)) + self.get_average((self._v,))
+            if cur_p <= 1.0 and cur_e < prev_e:
+                prev_e, prev_p = cur_e, cur_p
+                prev = self.rho.copy()
+            else:
+                self.rho = prev.copy()
+                dbeta *= 0.5
+                cur_e, cur_p = prev_e, prev_p
+        return self.rho
+
     def get_gibbs_state(self, kT, dbeta):
         """rho_bloch_cuda_1d.py:124-160 (delta initial state)."""
         nb = 1.0 / (kT * dbeta)

@@ -277,6 +277,32 @@ class WignerOracle:
                 break
         return self.W
 
+    def get_ground_state_cuda(self, dbeta, abs_tol_purity=1e-12):
+        """wigner_bloch_cuda_1d.py:167-227: imaginary-time steps from W = const,
+        each accepted only if purity <= 1, the energy <K> + <V> decreased and
+        sigma_x sigma_p >= 1/2; otherwise the previous state is restored and
+        dbeta halved.  Observables on the kernel grids (CUDA convention)."""
+        prev_e = cur_e = np.inf
+        prev_p = cur_p = 0.0
+        self.set_wignerfunction(np.full((self.Pn, self.Xn), 1.0 / (self.Pn * self.Xn)))
+        prev_W = self.W.copy()
+        X, P = self.X, self.P
+        t = self.t
+        while cur_p < (1.0 - abs_tol_purity) and dbeta > 1e-12:
+            self.bloch_single_step(dbeta)
+            cur_p = self.get_purity()
+            av = lambda F: np.sum(self.W * F) * self.dXdP  # noqa: E731
+            cur_e = av(np.broadcast_to(self._k(P, t), self.W.shape)) + av(np.broadcast_to(self._v(X, t), self.W.shape))
+            sig = np.sqrt((av(X * X + 0 * P) - av(X + 0 * P) ** 2) * (av(P * P + 0 * X) - av(P + 0 * X) ** 2))
+            if cur_p <= 1.0 and cur_e < prev_e and sig >= 0.5:
+                prev_e, prev_p = cur_e, cur_p
+                prev_W = self.W.copy()
+            else:
+                self.W = prev_W.copy()
+                dbeta *= 0.5
+                cur_e, cur_p = prev_e, prev_p
+        return self.W
+
     # -- random collision ------------------------------------------------------
     def setup_collision(self, gamma, kT, dbeta=0.01):
         """wigner_random_collision_model_fftw_1d.py:16-54 (W0 from the FFTW Bloch class)."""

@@ -2,13 +2,19 @@
 against the FP64 oracle (test infrastructure: imported by the GPU tests; run
 as a script it prints the tables as JSON).
 
-FP32 tolerances (complex64 spectra, FP64-built phases): 1e-5 relative L2 of
-W; per observable (rtol, atol) from FP32_OBS_TOL, about 3x the error of an
-exact complex64 numpy pipeline (W rounded to float32 after every pass) on
-the same cases.  Observables whose weight grows in the far tails (<V'> ~ x^3,
-<H>) inherit the FP32 round-off floor of W there multiplied by the weight
-(V(+-10) = 400 for the double well): the exact FP32 pipeline is already at
-4e-5 on -<V'> and 1.1e-4 on <H> for that case.  FP64: 1e-10 relative.
+FP32 tolerances (complex64 spectra, FP64-built phases).  Short runs (tens of
+steps): 1e-5 relative L2 of W; per observable (rtol, atol) from
+FP32_OBS_TOL, about 3x the error of a plain complex64 numpy pipeline (W
+rounded to float32 after every pass) on the same cases.  Observables whose
+weight grows in the far tails (<V'> ~ x^3, <H>) inherit the FP32 round-off
+floor of W there multiplied by the weight (V(+-10) = 400 for the double
+well).  Long runs: the error of any FP32 FFT pipeline grows linearly with the
+number of steps, because the rounded twiddles make every forward/inverse pair
+a fixed operator that differs from the exact one by O(1e-7) (on the 1024 x
+1024 double well: 2.9e-5 after 200 steps, 5.7e-4 after 4000, for numpy's
+pocketfft in complex64 as for these kernels).  Long-run tests therefore
+compare against complex64_pipeline on the same input and require the GPU
+error to stay within PIPELINE_FACTOR of it.  FP64: 1e-10 relative.
 
     python tests/parity_tables.py [--steps 4000] [--out table.json]
 """
@@ -36,6 +42,20 @@ FP32_OBS_TOL = {
     "hamiltonian_average": (5e-4, 3e-4),
 }
 OBS = tuple(FP32_OBS_TOL)
+PIPELINE_FACTOR = 2.0
+
+
+def within_pipeline(ours: dict, pipe: dict, factor: float = PIPELINE_FACTOR) -> list:
+    """Names of the quantities (W and each observable) whose error in `ours`
+    exceeds `factor` x the complex64 pipeline's error (plus 1e-12); both
+    dicts as returned by _errors."""
+    bad = []
+    if ours["W_rel_l2"] > factor * pipe["W_rel_l2"] + 1e-12:
+        bad.append("W")
+    for k in OBS:
+        if ours["obs"][k]["max_abs"] > factor * pipe["obs"][k]["max_abs"] + 1e-12:
+            bad.append(k)
+    return bad
 
 
 def ehrenfest_from_sums(o):
@@ -65,12 +85,14 @@ def _errors(got: dict, ref, W, Wref) -> dict:
     return out
 
 
-def config2_error_table(steps: int = 4000, seed: int = 11) -> dict:
+def config2_error_table(steps: int = 4000, seed: int = 11, with_pipeline: bool = True) -> dict:
     """The 1024 x 1024 double well (V = 0.05 x^4 - x^2, amplitudes 10/10,
     dt = 0.005, one Gaussian packet, x0 ~ U(-2, 2), p0 ~ U(-1, 1), width 0.5)
     propagated `steps` steps by the drop-in WignerMoyalFTTW1D in FP32 and in
     FP64 and by the FP64 oracle; returns the error of W and of every
-    Ehrenfest observable (max over the steps and at the last step)."""
+    Ehrenfest observable (max over the steps and at the last step), and the
+    same errors of the plain complex64 pipeline (complex64_pipeline), the
+    yardstick of the FP32 tolerance."""
     import bench
     import fastwigner_b200 as fw
     from oracle.wigner_oracle import WignerOracle
@@ -85,6 +107,10 @@ def config2_error_table(steps: int = 4000, seed: int = 11) -> dict:
     table = {"workload": f"double well {bench.GRID}x{bench.GRID}, dt={bench.DT}, {steps} steps, one packet "
                          f"(seed {seed}), drop-in WignerMoyalFTTW1D vs the FP64 oracle",
              "steps": steps}
+    if with_pipeline:
+        Wc, oc = complex64_pipeline(W0 / (W0.sum() * o.dXdP), steps, grid=bench.GRID, amp=bench.AMP, dt=bench.DT,
+                                    V=bench.V, K=bench.K, dV=bench.dV, dK=bench.dK)
+        table["complex64_pipeline"] = _errors(oc, o, Wc, o.W)
     for prec in ("float32", "float64"):
         q = fw.WignerMoyalFTTW1D(**kw, V=lambda _, x: bench.V(x), K=lambda _, p: bench.K(p),
                                  diff_V=lambda _, x: bench.dV(x), diff_K=lambda _, p: bench.dK(p), precision=prec)
@@ -92,6 +118,43 @@ def config2_error_table(steps: int = 4000, seed: int = 11) -> dict:
         W = np.asarray(q.propagate(steps), dtype=np.float64)
         table[prec] = _errors({k: getattr(q, k) for k in OBS}, o, W, o.W)
     return table
+
+
+def complex64_pipeline(W0, steps, *, grid, amp, dt, V, K, dV=None, dK=None):
+    """The same split-operator steps as the oracle, in a plain numpy complex64
+    pipeline (scipy.fft in single precision, the phase tables rounded once to
+    complex64, the state rounded to float32 after every pass): the error an
+    FP32 implementation of the algorithm makes without any compensation.
+    Returns the final state (float64 copy) and, with dV and dK, the Ehrenfest
+    observables of every step (FP64 sums of the FP32 state)."""
+    import scipy.fft as sf
+
+    dX = 2.0 * amp / grid
+    X = np.linspace(-amp, amp - dX, grid)[None, :]
+    P = np.linspace(-amp, amp - dX, grid)[:, None]
+    lam = np.fft.fftfreq(grid, dX / (2 * np.pi))[: grid // 2 + 1][None, :]
+    th = np.fft.fftfreq(grid, dX / (2 * np.pi))[: grid // 2 + 1][:, None]
+    eV = np.exp(-0.5j * dt * (V(X - th / 2) - V(X + th / 2))).astype(np.complex64)
+    eK = np.exp(-1j * dt * (K(P + lam / 2) - K(P - lam / 2))).astype(np.complex64)
+    W = np.asarray(W0, dtype=np.float32)
+    w = os.cpu_count()
+    obs = {k: [] for k in OBS}
+    for _ in range(steps):
+        W = sf.irfft(sf.rfft(W, axis=0, workers=w) * eV, n=grid, axis=0, workers=w).astype(np.float32)
+        W = sf.irfft(sf.rfft(W, axis=1, workers=w) * eK, n=grid, axis=1, workers=w).astype(np.float32)
+        W = sf.irfft(sf.rfft(W, axis=0, workers=w) * eV, n=grid, axis=0, workers=w).astype(np.float32)
+        W = (W / np.float32(W.astype(np.float64).sum() * dX * dX)).astype(np.float32)
+        if dV is not None:
+            W64 = W.astype(np.float64)
+            dc, dm = W64.sum(axis=0), W64.sum(axis=1)
+            dc, dm = dc / dc.sum(), dm / dm.sum()
+            x, p = X[0], P[:, 0]
+            obs["X_average"].append(dc @ x)
+            obs["P_average_RHS"].append(-(dc @ dV(x)))
+            obs["P_average"].append(dm @ p)
+            obs["X_average_RHS"].append(dm @ dK(p))
+            obs["hamiltonian_average"].append(dm @ K(p) + dc @ V(x))
+    return W.astype(np.float64), {k: np.array(v) for k, v in obs.items()}
 
 
 def main():
