@@ -67,6 +67,7 @@ _SIGNATURES = [
     ("fw_wigner_plan_create", c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(c_vp)]),
     ("fw_wigner_plan_destroy", c_int, [c_vp]),
     ("fw_wigner_num_obs", c_int, [c_int, c_int]),
+    ("fw_wigner_plan_status", c_int, [c_vp, ctypes.POINTER(c_int), c_int]),
     ("fw_wigner_propagate", c_int, [c_vp, ctypes.POINTER(WignerDesc), c_int, c_vp]),
     ("fw_wigner_weighted_sum", c_int, [c_vp, c_vp, c_ll, c_vp, c_vp, c_vp]),
     ("fw_wigner_propagate_timed", c_int, [c_vp, ctypes.POINTER(WignerDesc), c_int, c_vp,

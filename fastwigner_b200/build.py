@@ -22,6 +22,7 @@ BUILD = PKG / "_build"
 SOURCES = [
     "api.cu",
     "wigner_passes.cu",
+    "wigner_colp.cu",
     "rho_api.cu",
     "expr.cu",
     "fno.cu",

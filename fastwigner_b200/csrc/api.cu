@@ -82,6 +82,7 @@ struct fw_wigner_plan {
   void* wph = nullptr;  // spectra of the p-observable weights (wph_nb x 4 x P complex)
   int wph_nb = 0;
   double* tot = nullptr;  // per-instance reduced partial sums (batch x MMAX)
+  int* status = nullptr;  // device status word (FW_PASS_TIMEOUT); may be null
 };
 
 static constexpr int MMAX = 2 + 8;
@@ -126,6 +127,11 @@ extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wign
     cudaError_t e = cudaMalloc(&p->tot, sizeof(double) * (size_t)batch * MMAX);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(instance totals)");
   }
+  if (rc == FW_OK) {
+    cudaError_t e = cudaMalloc(&p->status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->status, 0, sizeof(int));
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc(plan status)");
+  }
   if (rc != FW_OK) {
     fw_wigner_plan_destroy(p);
     return rc;
@@ -143,7 +149,18 @@ extern "C" int fw_wigner_plan_destroy(fw_wigner_plan* p) {
   cudaFree(p->wsum);
   cudaFree(p->wph);
   cudaFree(p->tot);
+  cudaFree(p->status);
   delete p;
+  return FW_OK;
+}
+
+extern "C" int fw_wigner_plan_status(fw_wigner_plan* p, int* status_out, int clear) {
+  if (p == nullptr || status_out == nullptr) return fail(FW_EINVAL, "fw_wigner_plan_status: NULL argument");
+  *status_out = 0;
+  if (p->status == nullptr) return FW_OK;
+  cudaError_t e = cudaMemcpy(status_out, p->status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && clear) e = cudaMemset(p->status, 0, sizeof(int));
+  if (e != cudaSuccess) return cuda_fail(e, "fw_wigner_plan_status");
   return FW_OK;
 }
 
@@ -212,6 +229,7 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   base.blend_c = d->blend_c;
   base.out_scale = 1.0;
   base.small_shape = plan->small;
+  base.status = plan->status;
 
   auto tabV = [&](int k) { return advance(d->tabV, (long long)k * d->tabV_step, tes); };
   auto tabK = [&](int k) { return advance(d->tabK, (long long)k * d->tabK_step, tes); };

@@ -196,6 +196,7 @@ cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st) {
 }
 
 cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* nparts) {
+  if (colp_eligible(a, dtype)) return launch_col_persist(a, st, nparts);
 #define COLN(R, N) case N: return launch_col_n<R, N>(a, st, nparts);
   if (dtype == FW_F32) {
     switch (a.P) { COLN(float, 128) COLN(float, 256) COLN(float, 512) COLN(float, 1024) COLN(float, 2048) COLN(float, 4096) }

@@ -43,8 +43,9 @@ extern "C" {
 #define FW_ENVRTC 3   /* run-time compilation of a user expression failed */
 #define FW_ESTATE 4   /* handle in the wrong state */
 
-/* device status word of a batched launch (fw_batch_status) */
+/* device status words: of a batched launch (fw_batch_status) and of a plan (fw_wigner_plan_status) */
 #define FW_BATCH_TIMEOUT 1  /* a grid barrier gave up waiting; the launch returned early */
+#define FW_PASS_TIMEOUT 2   /* a pass's bulk copy into shared memory did not complete; its CTA returned early */
 
 /* step structure of fw_wigner_propagate */
 #define FW_STEP_FUSED 0 /* V/2 K V/2 with the closing V/2 of step n fused with the
@@ -74,6 +75,15 @@ typedef struct fw_wigner_plan fw_wigner_plan;
  */
 int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wigner_plan** out);
 int fw_wigner_plan_destroy(fw_wigner_plan* plan);
+
+/*
+ * Synchronous read of the plan's device status word (0, or FW_PASS_TIMEOUT
+ * when a pass gave up waiting for a bulk copy and its results are incomplete);
+ * clear != 0 resets it to 0 afterwards.  No reference counterpart (the
+ * reference's cuFFT calls report errors through their return status,
+ * cufft.py:95-102).
+ */
+int fw_wigner_plan_status(fw_wigner_plan* plan, int* status_out, int clear);
 
 /* Number of per-step observables (M) the plan writes for Mx x-weights and Mp p-weights: 2 + Mx + Mp.
  * Observable slots per instance and step: [sum W, sum W^2, sum W*wx_0(x) .., sum W*wp_0(p) ..]
