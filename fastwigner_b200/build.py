@@ -23,6 +23,7 @@ SOURCES = [
     "api.cu",
     "wigner_passes.cu",
     "wigner_colp.cu",
+    "wigner_rowp.cu",
     "rho_api.cu",
     "expr.cu",
     "fno.cu",

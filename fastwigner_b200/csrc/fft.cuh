@@ -261,4 +261,69 @@ template <typename Rl, int CP, int L> struct ColPadEx {
   __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
+// Exchange for the column passes with complex slots (one 8- or 16-byte access
+// per element instead of one per component): element i of FFT c at slot
+// (i + (i >> L)) * CP + c of one interleaved complex array, one pad slot per
+// 2^L elements (L = log2 RV), which keeps the Stockham and mid-point accesses
+// of 32/CP consecutive transform threads in distinct bank pairs and lets every
+// in-stage address fold into a per-thread base plus an immediate.  The array
+// holds (N + N/2^L) * CP complex values.  Synchronisation is CTA-wide.
+template <typename Rl, int CP, int L> struct ColPadExC {
+  cplx_t<Rl>* z;
+  int c;
+  using C = cplx_t<Rl>;
+  static constexpr int kL = L;
+  static constexpr bool kFold = true;
+  __device__ __forceinline__ int map(int i) const { return (i + (i >> L)) * CP + c; }
+  __device__ __forceinline__ static constexpr int delta(int d) { return (d + (d >> L)) * CP; }
+  __device__ __forceinline__ C read_at(int a) const { return z[a]; }
+  __device__ __forceinline__ void write_at(int a, C v) const { z[a] = v; }
+  __device__ __forceinline__ C read(int i) const { return read_at(map(i)); }
+  __device__ __forceinline__ void write(int i, C v) const { write_at(map(i), v); }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// Exchange for a group of T threads (one warp, T <= 32) that owns a private
+// buffer of N + N/32 complex slots (one pad slot per 32 elements, as GroupEx)
+// accessed one complex value at a time.  Warp-synchronous.
+template <typename Rl, int T> struct GroupExC {
+  cplx_t<Rl>* z;
+  using C = cplx_t<Rl>;
+  static_assert(T <= 32, "GroupExC is warp-synchronous");
+  static constexpr int kL = 5;
+  static constexpr bool kFold = true;
+  __device__ __forceinline__ static int map(int i) { return i + (i >> 5); }
+  __device__ __forceinline__ static constexpr int delta(int d) { return d + (d >> 5); }
+  __device__ __forceinline__ C read_at(int a) const { return z[a]; }
+  __device__ __forceinline__ void write_at(int a, C v) const { z[a] = v; }
+  __device__ __forceinline__ C read(int i) const { return read_at(map(i)); }
+  __device__ __forceinline__ void write(int i, C v) const { write_at(map(i), v); }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+
+// Sum NB complex values over the CP adjacent lanes of a row group (CP a power
+// of two, NB a multiple of CP) by recursive halving: at every level a lane
+// keeps one half of its current values, sends the other half to the partner
+// lane and adds what it receives, so the sum over CP lanes of NB values costs
+// 2 (NB - NB/CP) shuffles per lane instead of 2 NB log2(CP).  On return lane c
+// (= lane % CP) holds in u[0 .. NB/CP) the sums of entries c*NB/CP + i.
+template <int CP, int NB, typename C>
+__device__ __forceinline__ void halving_sum(C (&u)[NB], const int c) {
+  static_assert(NB % CP == 0, "halving_sum: NB must be a multiple of CP");
+#pragma unroll
+  for (int lv = 0; (CP >> (lv + 1)) >= 1; ++lv) {
+    const int off = CP >> (lv + 1);
+    const int half = NB >> (lv + 1);
+    const bool up = (c & off) != 0;
+#pragma unroll
+    for (int i = 0; i < half; ++i) {
+      C send = up ? u[i] : u[i + half];
+      const C keep = up ? u[i + half] : u[i];
+      send.x = __shfl_xor_sync(0xffffffffu, send.x, off);
+      send.y = __shfl_xor_sync(0xffffffffu, send.y, off);
+      u[i] = cadd(keep, send);
+    }
+  }
+}
+
 }  // namespace fw

@@ -38,6 +38,8 @@ cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st);
 cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P, int nb, void* out, long long out_bs,
                                int dtype, cudaStream_t st);
 bool colp_eligible(const PassArgs& a, int dtype);
+bool rowp_eligible(const PassArgs& a, int dtype);
+cudaError_t launch_row_persist(const PassArgs& a, cudaStream_t st);
 cudaError_t launch_col_persist(const PassArgs& a, cudaStream_t st, int* nparts);
 cudaError_t launch_totals(const double* part, int nparts, int M, int batch, double* tot, double* hist,
                           cudaStream_t st);

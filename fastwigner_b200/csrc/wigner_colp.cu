@@ -58,6 +58,7 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
   const C* G = reinterpret_cast<const C*>(a.wph) + (size_t)b * a.wph_bs;
   const bool obs = a.part_out != nullptr;
   const float h = (float)(0.5 / (double)N);
+  C u[RV];
   ex_write_natural<T, RV>(ex, j, v);
   ex.sync();
   o.s2 = 0;
@@ -90,17 +91,16 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
         o.ca = A.x;
         o.cb = Bi.y;
       }
-      if (a.Mp > 0) {
-        float ur = A.x + Bi.y, ui = A.y - Bi.x;
-#pragma unroll
-        for (int off = CP / 2; off > 0; off >>= 1) {
-          ur += __shfl_xor_sync(0xffffffffu, ur, off);
-          ui += __shfl_xor_sync(0xffffffffu, ui, off);
-        }
-        if (c == 0) psum[k] = mk<C>(ur, ui);
-      }
+      u[m] = mk<C>(A.x + Bi.y, A.y - Bi.x);  // 2 x (spectrum a + spectrum b)
     }
     v[m] = cscale(cadd(cmul(A, ea), cmul(Bi, eb)), h);
+  }
+  if (obs && a.Mp > 0) {
+    // per-bin sums over the tile's CP column pairs; lane c ends with bins
+    // m = c * RV/CP + i
+    halving_sum<CP, RV>(u, c);
+#pragma unroll
+    for (int i = 0; i < RV / CP; ++i) psum[j + (c * (RV / CP) + i) * T] = u[i];
   }
   ex.sync();
   if (obs && a.Mp > 0) {
@@ -185,8 +185,8 @@ __global__ void __launch_bounds__(CP* T, 1)
   const int c = tid % CP;
   const int j = tid / CP;
   __builtin_assume(j >= 0 && j < T);
-  using EXT = ColPadEx<float, CP, ilog2_c(RV)>;
-  EXT ex{exb, exb + (size_t)(N + T) * CP, c};
+  using EXT = ColPadExC<float, CP, ilog2_c(RV)>;
+  EXT ex{reinterpret_cast<C*>(exb), c};
 
   for (int it = first; it < last; ++it) {
     const int tile = item_t(it), b = item_b(it);
@@ -269,7 +269,7 @@ EncodeTiled encoder() {
 // FP32 3-D tensor map: dims {d0 (innermost), d1, d2}, byte strides of dims 1
 // and 2, box {b0, b1, 1}.
 bool encode_3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
-               uint32_t b0, uint32_t b1) {
+               uint32_t b0, uint32_t b1, CUtensorMapL2promotion promo) {
   EncodeTiled enc = encoder();
   if (enc == nullptr) return false;
   const cuuint64_t dims[3] = {d0, d1, d2};
@@ -277,8 +277,8 @@ bool encode_3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint6
   const cuuint32_t box[3] = {b0, b1, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
 }
 
 template <int N, int T, int CP>
@@ -293,9 +293,13 @@ cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
   const uint64_t wrow = (uint64_t)X * 4, winst = (uint64_t)a.w_bs * 4;
   const uint64_t trow = tab_cols * 4;
   const uint64_t tinst = a.tab_bs != 0 ? (uint64_t)a.tab_bs * (a.tab_real ? 4 : 8) : trow * (uint64_t)(P / 2 + 1);
-  if (!encode_3d(&mW, a.W, (uint64_t)X, (uint64_t)P, (uint64_t)a.batch, wrow, winst, 2 * CP, N < 256 ? N : 256) ||
+  // state rows of a tile are 2*CP floats: fetch exactly those sectors from DRAM
+  // (the neighbouring tile's half of each line is read by another CTA at
+  // another time); table rows are whole 128-byte lines
+  if (!encode_3d(&mW, a.W, (uint64_t)X, (uint64_t)P, (uint64_t)a.batch, wrow, winst, 2 * CP, N < 256 ? N : 256,
+                 CU_TENSOR_MAP_L2_PROMOTION_L2_64B) ||
       !encode_3d(&mT, a.tab1, tab_cols, (uint64_t)(P / 2 + 1), (uint64_t)ntab, trow, tinst, (uint32_t)tab_rowf,
-                 (uint32_t)TabBox<N>::ROWS))
+                 (uint32_t)TabBox<N>::ROWS, CU_TENSOR_MAP_L2_PROMOTION_L2_128B))
     return cudaErrorInvalidValue;
   auto kern = col_persist_kernel<N, T, CP>;
   static PerDeviceOnce attr;

@@ -185,6 +185,7 @@ int small_shapes(int dtype, int P, int X, int batch) {
 bool size_supported(int n) { return n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096; }
 
 cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st) {
+  if (rowp_eligible(a, dtype)) return launch_row_persist(a, st);
 #define ROWN(R, N) case N: return launch_row_n<R, N>(a, st);
   if (dtype == FW_F32) {
     switch (a.X) { ROWN(float, 128) ROWN(float, 256) ROWN(float, 512) ROWN(float, 1024) ROWN(float, 2048) ROWN(float, 4096) }
