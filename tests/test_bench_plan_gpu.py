@@ -85,7 +85,8 @@ def test_bench_plan_matches_oracle_every_instance(precision, steps):
             Wc, oc = complex64_pipeline(W0n[b], steps, grid=bench.GRID, amp=bench.AMP, dt=bench.DT, V=bench.V,
                                         K=bench.K, dV=bench.dV, dK=bench.dK)
             pipe = _errors(oc, o, Wc, o.W)
-            assert not within_pipeline(ours, pipe), (b, ours, pipe)
+            bad = within_pipeline(ours, pipe)
+            assert not bad, (b, bad)
             assert ours["W_rel_l2"] < 1e-4, b
         # the per-step norm sums the plan records are the un-normalised sums of a normalised state
         assert np.allclose(obs[:, b, 0] * sim.dXdP, 1.0, atol=1e-4 if precision == "float32" else 1e-10)
@@ -118,7 +119,8 @@ def test_config2_full_length_error_table():
     assert f64["W_rel_l2"] < 1e-10
     for k in OBS:
         assert f64["obs"][k]["max_abs"] <= 1e-10 * max(1.0, f64["obs"][k]["max_ref"]), k
-    assert not within_pipeline(f32, pipe), (f32, pipe)
+    bad = within_pipeline(f32, pipe)
+    assert not bad, bad
 
 
 def test_per_instance_tables_batch_matches_oracle():
