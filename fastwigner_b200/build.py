@@ -24,6 +24,7 @@ SOURCES = [
     "wigner_passes.cu",
     "wigner_colp.cu",
     "wigner_rowp.cu",
+    "wigner_generic.cu",
     "rho_api.cu",
     "expr.cu",
     "fno.cu",

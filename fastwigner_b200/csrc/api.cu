@@ -96,7 +96,7 @@ extern "C" int fw_wigner_plan_create(int P, int X, int batch, int dtype, fw_wign
   *out = nullptr;
   if (dtype != FW_F32 && dtype != FW_F64) return fail(FW_EINVAL, "fw_wigner_plan_create: dtype must be FW_F32 or FW_F64");
   if (!size_supported(P) || !size_supported(X))
-    return fail(FW_EINVAL, "fw_wigner_plan_create: P_gridDIM and X_gridDIM must be powers of two in [128, 4096] (got " +
+    return fail(FW_EINVAL, "fw_wigner_plan_create: P_gridDIM and X_gridDIM must be even and in [4, 4096] (got " +
                                std::to_string(P) + " x " + std::to_string(X) + ")");
   if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_plan_create: batch must be in [1, 65535]");
   const int small = small_shapes(dtype, P, X, batch);
@@ -288,7 +288,7 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
     // pair (observables from the mid-point spectrum) unless an x-p mask
     // (bxp) sits between them, or the p-weights change with the step or do
     // not fit the plan's spectrum buffer.
-    bool fuse = d->bxp == nullptr;
+    bool fuse = d->bxp == nullptr && !col_generic(plan->dtype, plan->P, plan->X);
     if (fuse && d->Mp > 0) {
       const int nb = d->wp_bstride != 0 ? B : 1;
       if (d->wp_step != 0 || plan->wph == nullptr || nb > plan->wph_nb) {
@@ -505,7 +505,7 @@ struct NoAllocLayout {
 int noalloc_layout(int P, int X, int batch, int dtype, const fw_wigner_desc* d, NoAllocLayout* L) {
   if (dtype != FW_F32 && dtype != FW_F64) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: bad dtype");
   if (!size_supported(P) || !size_supported(X))
-    return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: P and X must be powers of two in [128, 4096]");
+    return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: P and X must be even and in [4, 4096]");
   if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_wigner_propagate_noalloc: batch must be in [1, 65535]");
   L->small = small_shapes(dtype, P, X, batch);
   L->np = col_parts(dtype, P, X, L->small);

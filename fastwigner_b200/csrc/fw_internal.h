@@ -46,7 +46,14 @@ cudaError_t launch_totals(const double* part, int nparts, int M, int batch, doub
 int col_parts(int dtype, int P, int X, int small);
 int row_rv(int dtype, int N, int small);
 int small_shapes(int dtype, int P, int X, int batch);
+// Wigner plans: any even size in [4, 4096]; the register-resident passes take
+// the powers of two in [128, 4096], the others run the generic passes
 bool size_supported(int n);
+bool size_pow2_supported(int n);
+bool col_generic(int dtype, int P, int X);
+inline bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+cudaError_t launch_generic_row(const PassArgs& a, int dtype, cudaStream_t st);
+cudaError_t launch_generic_col(const PassArgs& a, int dtype, cudaStream_t st, int* nparts);
 
 void set_error(const std::string& msg);
 void count_launch(long long n);

@@ -69,7 +69,7 @@ extern "C" int fw_rho_plan_create(int N, int batch, int dtype, fw_rho_plan** out
   if (out == nullptr) return fail(FW_EINVAL, "fw_rho_plan_create: out is NULL");
   *out = nullptr;
   if (dtype != FW_F32 && dtype != FW_F64) return fail(FW_EINVAL, "fw_rho_plan_create: bad dtype");
-  if (!size_supported(N))
+  if (!size_pow2_supported(N))
     return fail(FW_EINVAL, "fw_rho_plan_create: X_gridDIM must be a power of two in [128, 4096] (got " +
                                std::to_string(N) + ")");
   if (batch < 1 || batch > 65535) return fail(FW_EINVAL, "fw_rho_plan_create: batch must be in [1, 65535]");

@@ -39,12 +39,28 @@ template <int N> struct TabBox {
   static constexpr int ROWS = (H + NL - 1) / NL;
 };
 
-template <int N, int T, int CP> struct ColpLayout {
+// Launch shapes of the persistent column pass.  MINB CTAs of CP*T threads per
+// SM.  BMAJOR: work items instance-major (consecutive items of a CTA are
+// neighbouring column tiles of one instance, so a tile whose rows are narrower
+// than a 64-byte DRAM line finds the rest of the line in L2; the table tile is
+// fetched for every item) instead of column-tile major (consecutive items share
+// the table tile).  PSUM_ALIAS: the per-bin p-weight sums live in the table
+// tile's buffer once the mid-point has read the table (only with a table fetch
+// per item).
+template <int N> struct ColpShape;
+template <> struct ColpShape<1024> {
+  static constexpr int T = 64, CP = 4, MINB = 2;
+  static constexpr bool BMAJOR = true, PSUM_ALIAS = true;
+};
+
+template <int N, int T, int CP, bool PSUM_ALIAS> struct ColpLayout {
   static constexpr int WROWB = 2 * CP;                        // floats per state-tile row
   static constexpr size_t W_FLOATS = (size_t)N * WROWB;
   static constexpr size_t T_FLOATS = (size_t)TabBox<N>::NL * TabBox<N>::ROWS * 4 * CP;  // complex tables
   static constexpr size_t EX_FLOATS = col_ex_reals<float, N, T, CP>();
-  static constexpr size_t BYTES = (W_FLOATS + T_FLOATS + EX_FLOATS) * 4 + (size_t)2 * N * 8;  // + twiddles + psum
+  static constexpr size_t PSUM_FLOATS = PSUM_ALIAS ? 0 : (size_t)2 * N;
+  static constexpr size_t BYTES = (W_FLOATS + T_FLOATS + EX_FLOATS + PSUM_FLOATS) * 4 + (size_t)N * 8;  // + twiddles
+  static_assert(!PSUM_ALIAS || T_FLOATS >= (size_t)2 * N, "psum must fit in the table buffer");
 };
 
 // Mid-point of the fused column pass with the phase-table tile in shared
@@ -95,15 +111,14 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
     }
     v[m] = cscale(cadd(cmul(A, ea), cmul(Bi, eb)), h);
   }
+  // per-bin sums over the tile's CP column pairs; lane c ends with bins
+  // m = c * RV/CP + i
+  if (obs && a.Mp > 0) halving_sum<CP, RV>(u, c);
+  ex.sync();  // the table tile and the exchange buffer are no longer read
   if (obs && a.Mp > 0) {
-    // per-bin sums over the tile's CP column pairs; lane c ends with bins
-    // m = c * RV/CP + i
-    halving_sum<CP, RV>(u, c);
 #pragma unroll
     for (int i = 0; i < RV / CP; ++i) psum[j + (c * (RV / CP) + i) * T] = u[i];
-  }
-  ex.sync();
-  if (obs && a.Mp > 0) {
+    ex.sync();
     for (int k = threadIdx.x; k < N; k += blockDim.x) {
       const C u = psum[k];
       C g[MAXO];
@@ -120,12 +135,12 @@ struct ColpCtl {
   int tab_inst;  // phase tables per instance (1) or one for the batch (0)
 };
 
-template <int N, int T, int CP>
-__global__ void __launch_bounds__(CP* T, 1)
+template <int N, int T, int CP, int MINB, bool BMAJOR, bool PSUM_ALIAS>
+__global__ void __launch_bounds__(CP* T, MINB)
     col_persist_kernel(const __grid_constant__ CUtensorMap mW, const __grid_constant__ CUtensorMap mT, PassArgs a,
                        ColpCtl ctl) {
   using C = float2;
-  using L = ColpLayout<N, T, CP>;
+  using L = ColpLayout<N, T, CP, PSUM_ALIAS>;
   constexpr int RV = N / T;
   constexpr int NTHR = CP * T;
   constexpr int WBOX = N < 256 ? N : 256;  // state rows per bulk copy
@@ -138,7 +153,7 @@ __global__ void __launch_bounds__(CP* T, 1)
   float* Ts = Ws + L::W_FLOATS;
   float* exb = Ts + L::T_FLOATS;
   C* tw = reinterpret_cast<C*>(exb + L::EX_FLOATS);
-  C* psum = tw + N;
+  C* psum = PSUM_ALIAS ? reinterpret_cast<C*>(Ts) : tw + N;
 
   const int n_items = a.batch * ctl.ntiles;
   const int first = (int)((long long)blockIdx.x * n_items / gridDim.x);
@@ -148,9 +163,11 @@ __global__ void __launch_bounds__(CP* T, 1)
   const int tab_rowf = (a.tab_real ? 2 : 4) * CP;  // floats per table-tile row
   const uint32_t w_bytes = (uint32_t)(L::W_FLOATS * 4);
   const uint32_t t_bytes = (uint32_t)(TabBox<N>::NL * TabBox<N>::ROWS * tab_rowf * 4);
-  auto item_t = [&](int it) { return it / a.batch; };
-  auto item_b = [&](int it) { return it % a.batch; };
-  auto tab_key = [&](int it) { return ctl.tab_inst ? it : item_t(it) * a.batch; };
+  auto item_t = [&](int it) { return BMAJOR ? it % ctl.ntiles : it / a.batch; };
+  auto item_b = [&](int it) { return BMAJOR ? it / ctl.ntiles : it % a.batch; };
+  // key of the table tile an item reads; with the p-weight sums in the table
+  // buffer every item fetches its tile
+  auto tab_key = [&](int it) { return (ctl.tab_inst || PSUM_ALIAS) ? it : item_t(it) * a.batch; };
   auto issue_w = [&](int it) {
     mbar_arrive_expect_tx(&bars[0], w_bytes);
 #pragma unroll
@@ -228,10 +245,13 @@ __global__ void __launch_bounds__(CP* T, 1)
     }
     MidSums<float> o;
     fused_mid_staged<N, T, RV, CP>(a, b, v, j, ex, c, Ts, psum, o);  // ends with a CTA barrier
-    t_pending = it + 1 < last && tab_key(it + 1) != tab_key(it);
-    if (tid == 0 && t_pending) issue_t(it + 1);
     const int xa = tile * 2 * CP + 2 * c;
     if (a.part_out != nullptr) mid_store<float, N, CP, NTHR>(a, b, tile, ctl.ntiles, o, xa, ored);
+    // the next item's table tile (the p-weight sums in the table buffer have
+    // been read before mid_store's barrier)
+    t_pending = it + 1 < last && tab_key(it + 1) != tab_key(it);
+    if (PSUM_ALIAS && a.part_out == nullptr) __syncthreads();  // no mid_store barrier to lean on
+    if (tid == 0 && t_pending) issue_t(it + 1);
     // ---- inverse transform and store
     fft<N, T, RV, +1, C, EXT>(v, j, ex, tw);
     float* W = reinterpret_cast<float*>(a.W) + (size_t)b * a.w_bs;
@@ -281,9 +301,11 @@ bool encode_3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint6
          CUDA_SUCCESS;
 }
 
-template <int N, int T, int CP>
+template <int N>
 cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
-  using L = ColpLayout<N, T, CP>;
+  using S = ColpShape<N>;
+  constexpr int T = S::T, CP = S::CP;
+  using L = ColpLayout<N, T, CP, S::PSUM_ALIAS>;
   const int P = a.P, X = a.X;
   const int ntiles = X / (2 * CP);
   const int tab_rowf = (a.tab_real ? 2 : 4) * CP;
@@ -301,7 +323,7 @@ cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
       !encode_3d(&mT, a.tab1, tab_cols, (uint64_t)(P / 2 + 1), (uint64_t)ntab, trow, tinst, (uint32_t)tab_rowf,
                  (uint32_t)TabBox<N>::ROWS, CU_TENSOR_MAP_L2_PROMOTION_L2_128B))
     return cudaErrorInvalidValue;
-  auto kern = col_persist_kernel<N, T, CP>;
+  auto kern = col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS>;
   static PerDeviceOnce attr;
   cudaError_t e = set_smem_once(attr, kern, L::BYTES);
   if (e != cudaSuccess) return e;
@@ -309,7 +331,8 @@ cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   ColpCtl ctl{ntiles, a.tab_bs != 0 ? 1 : 0};
   const int items = a.batch * ntiles;
-  const int grid = items < sms ? items : sms;
+  const int ctas = sms * S::MINB;
+  const int grid = items < ctas ? items : ctas;
   kern<<<grid, CP * T, L::BYTES, st>>>(mW, mT, a, ctl);
   if (nparts) *nparts = ntiles;
   return cudaGetLastError();
@@ -328,15 +351,17 @@ bool colp_eligible(const PassArgs& a, int dtype) {
   if (a.bxp != nullptr || a.blend_pre || a.blend_post || a.small_shape) return false;
   if (a.P != 1024) return false;
   const uintptr_t mis = reinterpret_cast<uintptr_t>(a.W) | reinterpret_cast<uintptr_t>(a.tab1);
-  if ((mis & 15) != 0 || (a.w_bs % 4) != 0 || (a.X % 16) != 0) return false;
+  if ((mis & 15) != 0 || (a.w_bs % 4) != 0) return false;
   if (a.tab_bs != 0 && (a.tab_bs * (a.tab_real ? 4 : 8)) % 16 != 0) return false;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (long long)a.batch * (a.X / 16) >= 2LL * sms && encoder() != nullptr;
+  using S = ColpShape<1024>;
+  if (a.X % (2 * S::CP) != 0 || col_parts(dtype, a.P, a.X, 0) != a.X / (2 * S::CP)) return false;
+  return (long long)a.batch * (a.X / (2 * S::CP)) >= 2LL * S::MINB * sms && encoder() != nullptr;
 }
 
 cudaError_t launch_col_persist(const PassArgs& a, cudaStream_t st, int* nparts) {
-  return launch_colp_cfg<1024, 64, 8>(a, st, nparts);
+  return launch_colp_cfg<1024>(a, st, nparts);
 }
 
 }  // namespace fw

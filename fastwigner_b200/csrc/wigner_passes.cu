@@ -83,7 +83,9 @@ template <> struct RowCfg<double, 4096> { static constexpr int T = 256, G = 1, M
 template <> struct ColCfg<float, 128> { static constexpr int T = 16, CP = 32, MINB = 1; };
 template <> struct ColCfg<float, 256> { static constexpr int T = 32, CP = 16, MINB = 1; };
 template <> struct ColCfg<float, 512> { static constexpr int T = 32, CP = 16, MINB = 1; };
-template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 8, MINB = 1; };
+// 1024: four column pairs, two CTAs per SM -- the tile of the persistent
+// column pass (wigner_colp.cu), which writes the same partial-sum records
+template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 4, MINB = 2; };
 template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 4, MINB = 1; };
 template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 2, MINB = 1; };
 template <> struct ColCfg<double, 128> { static constexpr int T = 16, CP = 16, MINB = 1; };
@@ -152,8 +154,29 @@ static cudaError_t launch_col_n(const PassArgs& a, cudaStream_t st, int* nparts)
   return launch_col_cfg<Rl, N, Cfg::T, Cfg::CP, Cfg::MINB>(a, st, nparts);
 }
 
-// Partial-sum records per instance of a plan's column passes: X / (2 CP).
+// Column passes of sizes the register-resident kernels do not take (P not a
+// power of two in [128, 4096], or X not a multiple of their column tile) run
+// the generic pass, one column pair per CTA.
+static int col_cp(int dtype, int P, int small) {
+  int cp = 0;
+#define CPV(R, N) if (P == N) cp = small ? ColCfgSmall<R, N>::CP : ColCfg<R, N>::CP;
+  if (dtype == FW_F32) { CPV(float, 128) CPV(float, 256) CPV(float, 512) CPV(float, 1024) CPV(float, 2048) CPV(float, 4096) }
+  else { CPV(double, 128) CPV(double, 256) CPV(double, 512) CPV(double, 1024) CPV(double, 2048) CPV(double, 4096) }
+#undef CPV
+  return cp;
+}
+
+bool col_generic(int dtype, int P, int X) {
+  const int cp = col_cp(dtype, P, 0);
+  const int cps = col_cp(dtype, P, 1);
+  return cp == 0 || X % (2 * cp) != 0 || X % (2 * cps) != 0;
+}
+
+// Partial-sum records per instance of a plan's column passes: X / (2 CP), or
+// X / 2 for the generic pass.
 int col_parts(int dtype, int P, int X, int small) {
+  if (X < 2 || X % 2 != 0) return -1;
+  if (col_generic(dtype, P, X)) return X / 2;
   int cp = 0;
 #define CPV(R, N) if (P == N) cp = small ? ColCfgSmall<R, N>::CP : ColCfg<R, N>::CP;
   if (dtype == FW_F32) { CPV(float, 128) CPV(float, 256) CPV(float, 512) CPV(float, 1024) CPV(float, 2048) CPV(float, 4096) }
@@ -166,6 +189,7 @@ int col_parts(int dtype, int P, int X, int small) {
 // Values per thread of the row pass transform of length N (the radix plan
 // its stage-layout twiddle table is built for).
 int row_rv(int dtype, int N, int small) {
+  if (!size_pow2_supported(N)) return 0;  // generic row pass: k-indexed twiddles
   int t = 0;
 #define RT(R, N_) if (N == N_) t = small ? RowCfgSmall<R, N_>::T : RowCfg<R, N_>::T;
   if (dtype == FW_F32) { RT(float, 128) RT(float, 256) RT(float, 512) RT(float, 1024) RT(float, 2048) RT(float, 4096) }
@@ -176,15 +200,18 @@ int row_rv(int dtype, int N, int small) {
 // Small-batch shapes when the column pass with the regular shapes would have
 // fewer CTAs than the GPU has SMs.
 int small_shapes(int dtype, int P, int X, int batch) {
+  if (col_generic(dtype, P, X) || !size_pow2_supported(X)) return 0;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int np = col_parts(dtype, P, X, 0);
   return np > 0 && (long long)batch * np < sms ? 1 : 0;
 }
 
-bool size_supported(int n) { return n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096; }
+bool size_pow2_supported(int n) { return n == 128 || n == 256 || n == 512 || n == 1024 || n == 2048 || n == 4096; }
+bool size_supported(int n) { return n >= 4 && n <= 4096 && n % 2 == 0; }
 
 cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st) {
+  if (!size_pow2_supported(a.X)) return launch_generic_row(a, dtype, st);
   if (rowp_eligible(a, dtype)) return launch_row_persist(a, st);
 #define ROWN(R, N) case N: return launch_row_n<R, N>(a, st);
   if (dtype == FW_F32) {
@@ -197,6 +224,7 @@ cudaError_t launch_row(const PassArgs& a, int dtype, cudaStream_t st) {
 }
 
 cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* nparts) {
+  if (col_generic(dtype, a.P, a.X)) return launch_generic_col(a, dtype, st, nparts);
   if (colp_eligible(a, dtype)) return launch_col_persist(a, st, nparts);
 #define COLN(R, N) case N: return launch_col_n<R, N>(a, st, nparts);
   if (dtype == FW_F32) {

@@ -6,11 +6,12 @@
 // pipeline over a contiguous range of (row pair, instance) work items: the
 // next item's two rows (8 KiB at X = 1024) arrive in the warp's shared-memory
 // staging buffer by a bulk copy issued as soon as the current rows are in
-// registers, and the two rows of the phase table the item needs arrive the
-// same way after the current spectral multiply has read its own (items are
-// row-pair major, so with one table for the batch a warp fetches a table pair
-// once per row pair it visits).  The stage twiddles live in shared memory for
-// the life of the CTA.  Copies are plain bulk loads from this GPU's own
+// registers, so the copy overlaps the item's whole transform pair.  The two
+// rows of the phase table an item needs can be staged the same way
+// (kRowStageTable; items are row-pair major, so with one table for the batch a
+// warp would fetch a table pair once per row pair it visits), or read from L2
+// during the spectral multiply, which leaves room for more warps per SM.  The
+// stage twiddles live in shared memory for the life of the CTA.  Copies are plain bulk loads from this GPU's own
 // memory; every wait is bounded (FW_PASS_TIMEOUT in the plan status word, then
 // the warp returns).
 #include "fw_internal.h"
@@ -20,13 +21,17 @@
 namespace fw {
 
 constexpr long long kRowMaxPolls = 1LL << 22;
-constexpr int kRowWarps = 8;  // warps (independent pipelines) per CTA, one CTA per SM
+// warps (independent pipelines) per CTA, one CTA per SM: 12 x 168 registers
+// fill the register file; the phase-table rows are then read from L2 (a
+// warp-private staged copy would leave room for 8 warps only)
+constexpr int kRowWarps = 12;
+constexpr bool kRowStageTable = false;
 
 template <int N> struct RowpLayout {
   static constexpr int T = 32, RV = N / T;
-  static constexpr size_t W_BYTES = (size_t)2 * N * 4;          // the item's two rows
-  static constexpr size_t T_BYTES = (size_t)2 * (N / 2 + 1) * 8;  // their two complex table rows
-  static constexpr size_t EX_BYTES = (size_t)(N + N / 32) * 8;    // GroupExC exchange buffer
+  static constexpr size_t W_BYTES = (size_t)2 * N * 4;                                  // the item's two rows
+  static constexpr size_t T_BYTES = kRowStageTable ? (size_t)2 * (N / 2 + 1) * 8 : 0;  // their two table rows
+  static constexpr size_t EX_BYTES = (size_t)(N + N / 32) * 8;                          // GroupExC exchange
   static constexpr size_t WARP_BYTES = ((W_BYTES + T_BYTES + EX_BYTES + 127) / 128) * 128;
   static constexpr int STW = stage_off(N, RV, N);  // stage-layout twiddles (complex entries)
   static constexpr size_t BYTES = (size_t)kRowWarps * WARP_BYTES + (size_t)STW * 8;
@@ -74,10 +79,10 @@ __global__ void __launch_bounds__(32 * kRowWarps, 1) row_persist_kernel(PassArgs
   };
   if (lane == 0) {
     issue_w(first);
-    issue_t(first);
+    if (kRowStageTable) issue_t(first);
   }
   uint32_t ph_w = 0, ph_t = 0;
-  bool w_pending = true, t_pending = true, failed = false;
+  bool w_pending = true, t_pending = kRowStageTable, failed = false;
   GroupExC<float, T> ex{exz};
   const int j = lane;
   const float f = (float)(a.out_scale / (double)N);
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(32 * kRowWarps, 1) row_persist_kernel(PassArgs
     }
     fft<N, T, RV, -1, C, GroupExC<float, T>, true>(v, j, ex, tws);
     // ---- exp(K) from the staged table rows (Hermitian-unpacked pair multiply)
-    if (t_pending) {
+    if (kRowStageTable && t_pending) {
       if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[w][1], ph_t, kRowMaxPolls))) {
         failed = true;
         break;
@@ -116,17 +121,20 @@ __global__ void __launch_bounds__(32 * kRowWarps, 1) row_persist_kernel(PassArgs
     }
     ex_write_natural<T, RV>(ex, j, v);
     ex.sync();
+    const C* tab = kRowStageTable
+                       ? Ts
+                       : reinterpret_cast<const C*>(a.tab1) + (size_t)b * a.tab_bs + (size_t)(2 * rp) * HS;
 #pragma unroll
     for (int m = 0; m < RV; ++m) {
       const int k = j + m * T;
       const int kk = (k <= N / 2) ? k : N - k;
-      const C ea = herm(Ts[kk], k, N);
-      const C eb = herm(Ts[HS + kk], k, N);
+      const C ea = herm(kRowStageTable ? tab[kk] : __ldg(tab + kk), k, N);
+      const C eb = herm(kRowStageTable ? tab[HS + kk] : __ldg(tab + HS + kk), k, N);
       const C znk = ex.read((N - k) & (N - 1));
       v[m] = two_real_mul(v[m], znk, ea, eb, f);
     }
     ex.sync();  // every lane is done with Ts and the exchange buffer
-    if (it + 1 < last && tkey(it + 1) != tkey(it)) {
+    if (kRowStageTable && it + 1 < last && tkey(it + 1) != tkey(it)) {
       if (lane == 0) issue_t(it + 1);
       t_pending = true;
     }

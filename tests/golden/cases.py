@@ -69,6 +69,30 @@ CASES = {
         kw=dict(t=0.0, dt=0.01, X_gridDIM=128, X_amplitude=8.0, P_gridDIM=128, P_amplitude=7.0, gamma=0.5, kT=0.5,
                 **HARMONIC),
         init=coherent(1.5, -0.5), steps=20),
+    # even sizes that are not powers of two (the reference only asserts evenness):
+    # 96 = 4^2 2 3, 192 = 4^3 3, 100 = 4 5^2, 160 = 4^2 2 5, 98 = 2 7^2, 202 = 2 101
+    "moyal_dw_96x192": dict(
+        cls="WignerMoyalFTTW1D",
+        kw=dict(t=0.0, dt=0.005, X_gridDIM=192, X_amplitude=10.0, P_gridDIM=96, P_amplitude=10.0, **DOUBLE_WELL),
+        init=coherent(-1.3, 0.4, 0.5), steps=30),
+    "moyal_harmonic_100": dict(
+        cls="WignerMoyalFTTW1D",
+        kw=dict(t=0.0, dt=0.01, X_gridDIM=100, X_amplitude=8.0, P_gridDIM=100, P_amplitude=7.0, **HARMONIC),
+        init=coherent(1.0, 0.5), steps=20),
+    "moyal_dw_98x202": dict(
+        cls="WignerMoyalFTTW1D",
+        kw=dict(t=0.0, dt=0.005, X_gridDIM=202, X_amplitude=10.0, P_gridDIM=98, P_amplitude=10.0, alpha=0.5,
+                **DOUBLE_WELL),
+        init=coherent(0.8, -0.3, 0.5), steps=15),
+    "bloch_fftw_harmonic_160": dict(
+        cls="WignerBlochFFTW1D",
+        kw=dict(t=0.0, dt=0.01, X_gridDIM=160, X_amplitude=8.0, P_gridDIM=160, P_amplitude=7.0, kT=0.5,
+                dbeta=0.01, K=lambda _, p: 0.5 * p ** 2, V=lambda _, x: 0.5 * x ** 2)),
+    "collision_harmonic_96": dict(
+        cls="WignerRandomCollisionModelFFTW1D",
+        kw=dict(t=0.0, dt=0.01, X_gridDIM=96, X_amplitude=8.0, P_gridDIM=96, P_amplitude=7.0, gamma=0.5, kT=0.5,
+                **HARMONIC),
+        init=coherent(1.5, -0.5), steps=20),
 }
 
 # The configuration-1 workload at full size; only observables are stored.

@@ -35,6 +35,11 @@ def test_abi_version_and_error_path():
     lib = _lib.load()
     assert lib.fw_abi_version() == _lib.FW_ABI_VERSION
     out = _lib.c_vp()
-    rc = lib.fw_wigner_plan_create(100, 128, 1, _lib.FW_F32, ctypes.byref(out))
-    assert rc == 1  # FW_EINVAL, checked before any device work
-    assert b"powers of two" in lib.fw_last_error()
+    rc = lib.fw_wigner_plan_create(101, 128, 1, _lib.FW_F32, ctypes.byref(out))
+    assert rc == 1  # FW_EINVAL (odd size, as the reference asserts), checked before any device work
+    assert b"must be even" in lib.fw_last_error()
+    rc = lib.fw_wigner_plan_create(128, 8192, 1, _lib.FW_F32, ctypes.byref(out))
+    assert rc == 1  # beyond the largest transform length
+    rc = lib.fw_rho_plan_create(100, 1, _lib.FW_F64, ctypes.byref(out))
+    assert rc == 1  # density-matrix plans: powers of two only
+    assert b"power of two" in lib.fw_last_error()
