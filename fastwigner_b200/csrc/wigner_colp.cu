@@ -32,11 +32,15 @@ namespace fw {
 constexpr long long kTmaMaxPolls = 1LL << 22;  // polls of one mbarrier wait before the CTA gives up
 
 // Rows of the phase-table tile one bulk copy moves, and the copies per tile
-// (a box dimension may not exceed 256).
+// (a box dimension may not exceed 256).  ROWS is a multiple of 4, so that
+// every copy's shared-memory destination (ROWS rows of 32, 64 or 128 bytes)
+// starts on 128 bytes; the last copy may run past the table's N/2+1 rows,
+// which the copy fills with zeros.
 template <int N> struct TabBox {
   static constexpr int H = N / 2 + 1;
   static constexpr int NL = (H + 255) / 256;
-  static constexpr int ROWS = (H + NL - 1) / NL;
+  static constexpr int ROWS = ((H + NL - 1) / NL + 3) / 4 * 4;
+  static_assert(ROWS <= 256, "table box too tall");
 };
 
 // Launch shapes of the persistent column pass.  MINB CTAs of CP*T threads per
@@ -59,8 +63,15 @@ template <int N, int T, int CP, bool PSUM_ALIAS> struct ColpLayout {
   static constexpr size_t T_FLOATS = (size_t)TabBox<N>::NL * TabBox<N>::ROWS * 4 * CP;  // complex tables
   static constexpr size_t EX_FLOATS = col_ex_reals<float, N, T, CP>();
   static constexpr size_t PSUM_FLOATS = PSUM_ALIAS ? 0 : (size_t)2 * N;
-  static constexpr size_t BYTES = (W_FLOATS + T_FLOATS + EX_FLOATS + PSUM_FLOATS) * 4 + (size_t)N * 8;  // + twiddles
+  // + twiddles, + 128 bytes to align the base of the buffers
+  static constexpr size_t BYTES = (W_FLOATS + T_FLOATS + EX_FLOATS + PSUM_FLOATS) * 4 + (size_t)N * 8 + 128;
   static_assert(!PSUM_ALIAS || T_FLOATS >= (size_t)2 * N, "psum must fit in the table buffer");
+  // every bulk-tensor destination on 128 bytes: the state boxes, the table
+  // buffer and each table box (complex and real tables)
+  static_assert((W_FLOATS * 4) % 128 == 0 && ((size_t)(N < 256 ? N : 256) * WROWB * 4) % 128 == 0,
+                "state boxes off 128 bytes");
+  static_assert(((size_t)TabBox<N>::ROWS * 4 * CP * 4) % 128 == 0 && ((size_t)TabBox<N>::ROWS * 2 * CP * 4) % 128 == 0,
+                "table boxes off 128 bytes");
 };
 
 // Mid-point of the fused column pass with the phase-table tile in shared
@@ -144,11 +155,13 @@ __global__ void __launch_bounds__(CP* T, MINB)
   constexpr int RV = N / T;
   constexpr int NTHR = CP * T;
   constexpr int WBOX = N < 256 ? N : 256;  // state rows per bulk copy
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t bars[2];  // [0] state tile, [1] table tile
   __shared__ double red[34];
   __shared__ double ored[NTHR / 32][2 + 2 * MAXO];
   __shared__ int abort_flag;
+  // bulk-tensor copies land on 128-byte boundaries: align the buffers' base
+  unsigned char* smem = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
   float* Ws = reinterpret_cast<float*>(smem);
   float* Ts = Ws + L::W_FLOATS;
   float* exb = Ts + L::T_FLOATS;

@@ -34,7 +34,7 @@ template <int N> struct RowpLayout {
   static constexpr size_t EX_BYTES = (size_t)(N + N / 32) * 8;                          // GroupExC exchange
   static constexpr size_t WARP_BYTES = ((W_BYTES + T_BYTES + EX_BYTES + 127) / 128) * 128;
   static constexpr int STW = stage_off(N, RV, N);  // stage-layout twiddles (complex entries)
-  static constexpr size_t BYTES = (size_t)kRowWarps * WARP_BYTES + (size_t)STW * 8;
+  static constexpr size_t BYTES = (size_t)kRowWarps * WARP_BYTES + (size_t)STW * 8 + 128;  // + base alignment
 };
 
 template <int N>
@@ -43,8 +43,9 @@ __global__ void __launch_bounds__(32 * kRowWarps, 1) row_persist_kernel(PassArgs
   using L = RowpLayout<N>;
   constexpr int T = 32, RV = N / T;
   constexpr size_t HS = N / 2 + 1;
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t bars[kRowWarps][2];  // per warp: [0] rows, [1] table rows
+  unsigned char* smem = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);  // 128-byte aligned base
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* mine = smem + (size_t)w * L::WARP_BYTES;
   float* Ws = reinterpret_cast<float*>(mine);
