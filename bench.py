@@ -142,6 +142,30 @@ def parity_check(sim, W0, steps=20):
             "against": "FP64 oracle (numpy restatement of WignerMoyalFTTW1D.propagate)", "tol_rel_l2": 1e-5}
 
 
+# The other configurations (fastwigner_b200/benchmarks.py), measured after the
+# headline on the same GPU so that every run records them: config 1 (FP64 Moyal
+# 256^2), config 2b (von Neumann complex64 1024^2), config 3 (Bloch 512^2 Morse
+# batch), config 4 (uneven persistent batch) and config 5 (strong field with
+# collisions).  Each entry is that workload's own line, trimmed.
+OTHER_WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field")
+
+
+def other_workloads():
+    from fastwigner_b200 import benchmarks
+
+    out = {}
+    for name in OTHER_WORKLOADS:
+        try:
+            line = benchmarks.run(name)
+            out[name] = {"value": line["value"], "unit": line["unit"], "ms_per_step": line["ms_per_step"],
+                         "dtype": line["dtype"], "roofline_frac": line["roofline"]["frac"],
+                         "algorithmic_bytes_per_unit": line["roofline"]["algorithmic_bytes_per_unit"],
+                         "clocks_sm_mhz": line["clocks"].get("sm_mhz"), "config": line["config"]}
+        except Exception as e:  # a failing side workload must not cost the headline line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
 # ---------------------------------------------------------------------------
 def cpu_reference_rate(target_s, steps=None, grid=GRID, workers=None):
     """Time the FP64 oracle port (the reference algorithm; FFTs on `workers`
@@ -317,6 +341,7 @@ def run_ours(args):
     d2h = (host_out[0].numel() * 4 + obs_host[0].numel() * 8) / E2E_STEPS
 
     parity = parity_check(sim, W0_pinned) if rank == 0 else None
+    others = other_workloads() if rank == 0 and world == 1 and not args.no_workloads else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -343,6 +368,7 @@ def run_ours(args):
                        "e2e_finite": e2e_finite},
             "roofline": roofline,
             "parity": parity,
+            "workloads": others,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -363,6 +389,7 @@ def main():
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the other configurations' figures")
     ap.add_argument("--workload", default="moyal_1024",
                     help="moyal_1024 (the default line) or one of fastwigner_b200.benchmarks.WORKLOADS")
     args = ap.parse_args()

@@ -304,15 +304,18 @@ template <typename Rl>
 static cudaError_t gen_launch(const PassArgs& a, bool row, cudaStream_t st, int* nparts) {
   const int N = row ? a.X : a.P;
   const size_t smem = (size_t)2 * N * sizeof(cplx_t<Rl>);
+  // the attribute is the largest dynamic shared memory any launch of the
+  // kernel may use (N up to 4096), not this launch's
+  const size_t smem_max = (size_t)2 * 4096 * sizeof(cplx_t<Rl>);
   const GenFactors g = gen_factors(N);
   if (row) {
     static PerDeviceOnce attr;
-    cudaError_t e = set_smem_once(attr, gen_row_kernel<Rl>, smem);
+    cudaError_t e = set_smem_once(attr, gen_row_kernel<Rl>, smem_max);
     if (e != cudaSuccess) return e;
     gen_row_kernel<Rl><<<dim3(a.P / 2, a.batch), kGenThreads, smem, st>>>(a, g);
   } else {
     static PerDeviceOnce attr;
-    cudaError_t e = set_smem_once(attr, gen_col_kernel<Rl>, smem);
+    cudaError_t e = set_smem_once(attr, gen_col_kernel<Rl>, smem_max);
     if (e != cudaSuccess) return e;
     gen_col_kernel<Rl><<<dim3(a.X / 2, a.batch), kGenThreads, smem, st>>>(a, g);
     if (nparts) *nparts = a.X / 2;

@@ -83,9 +83,9 @@ template <> struct RowCfg<double, 4096> { static constexpr int T = 256, G = 1, M
 template <> struct ColCfg<float, 128> { static constexpr int T = 16, CP = 32, MINB = 1; };
 template <> struct ColCfg<float, 256> { static constexpr int T = 32, CP = 16, MINB = 1; };
 template <> struct ColCfg<float, 512> { static constexpr int T = 32, CP = 16, MINB = 1; };
-// 1024: four column pairs, two CTAs per SM -- the tile of the persistent
-// column pass (wigner_colp.cu), which writes the same partial-sum records
-template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 4, MINB = 2; };
+// 1024: the column tile of the persistent column pass (wigner_colp.cu), which
+// writes the same partial-sum records
+template <> struct ColCfg<float, 1024> { static constexpr int T = 64, CP = 8, MINB = 1; };
 template <> struct ColCfg<float, 2048> { static constexpr int T = 64, CP = 4, MINB = 1; };
 template <> struct ColCfg<float, 4096> { static constexpr int T = 128, CP = 2, MINB = 1; };
 template <> struct ColCfg<double, 128> { static constexpr int T = 16, CP = 16, MINB = 1; };

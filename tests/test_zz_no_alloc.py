@@ -154,7 +154,7 @@ def test_noalloc_scratch_query_and_rejection():
     need = lib.fw_noalloc_scratch_needed(256, 256, 3, _lib.FW_F64, ctypes.byref(d))
     assert 0 < need <= fixed
     assert lib.fw_noalloc_scratch_needed(256, 256, 3, _lib.FW_F64, None) < need  # no weight spectra
-    assert lib.fw_noalloc_scratch_needed(100, 256, 3, _lib.FW_F64, None) == 0
+    assert lib.fw_noalloc_scratch_needed(101, 256, 3, _lib.FW_F64, None) == 0  # odd: rejected
     big = lib.fw_noalloc_scratch_needed(4096, 4096, 60000, _lib.FW_F64, ctypes.byref(d))
     assert big > fixed
     rc = lib.fw_wigner_propagate_noalloc(4096, 4096, 60000, _lib.FW_F64, ctypes.byref(d), 1, None)
