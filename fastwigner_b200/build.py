@@ -28,6 +28,7 @@ SOURCES = [
     "rho_api.cu",
     "expr.cu",
     "fno.cu",
+    "fno_umma.cu",
     "batch.cu",
 ]
 

@@ -235,6 +235,12 @@ extern "C" int fw_fno_sgemm(int transA, int transB, int M, int N, int K, float a
   if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return fail(FW_EINVAL, "fw_fno_sgemm: non-positive size");
   if (A == nullptr || B == nullptr || C == nullptr) return fail(FW_EINVAL, "fw_fno_sgemm: NULL operand");
   if (batch > 65535) return fail(FW_EINVAL, "fw_fno_sgemm: batch > 65535");
+  if (umma_gemm_eligible(M, N, K)) {  // tensor cores (tcgen05, three-way TF32 split)
+    cudaError_t e = launch_umma_gemm(transA, transB, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc,
+                                     strideC, batch, static_cast<cudaStream_t>(stream));
+    count_launch(1);
+    return e == cudaSuccess ? FW_OK : cuda_fail(e, "fw_fno_sgemm (tensor cores)");
+  }
   dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, batch);
   sgemm_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(transA, transB, M, N, K, alpha, A, lda, strideA, B,
                                                                      ldb, strideB, beta, C, ldc, strideC);
@@ -303,4 +309,9 @@ extern "C" int fw_fno_features(int Bn, int NP, int G0, int G1, const float* para
   count_launch(1);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FW_OK : cuda_fail(e, "fw_fno_features");
+}
+
+extern "C" int fw_fno_status(int* status_out, int clear) {
+  if (status_out == nullptr) return fail(FW_EINVAL, "fw_fno_status: NULL argument");
+  return fno_status_read(status_out, clear);
 }

@@ -46,6 +46,7 @@ extern "C" {
 /* device status words: of a batched launch (fw_batch_status) and of a plan (fw_wigner_plan_status) */
 #define FW_BATCH_TIMEOUT 1  /* a grid barrier gave up waiting; the launch returned early */
 #define FW_PASS_TIMEOUT 2   /* a pass's bulk copy into shared memory did not complete; its CTA returned early */
+#define FW_FNO_TIMEOUT 3    /* a tensor-core GEMM of the FNO gave up waiting for its MMAs; its tile holds NaN */
 
 /* step structure of fw_wigner_propagate */
 #define FW_STEP_FUSED 0 /* V/2 K V/2 with the closing V/2 of step n fused with the
@@ -337,10 +338,15 @@ int fw_batch_set_spin_limit(fw_batch* batch, long long polls);
 /* ------------------------------------------------------------------------ */
 
 /* C[b] = alpha op(A[b]) op(B[b]) + beta C[b]; op(A) M x K, op(B) K x N, row-major,
- * leading dimensions lda/ldb/ldc, batch strides strideA/B/C (elements), batch <= 65535. */
+ * leading dimensions lda/ldb/ldc, batch strides strideA/B/C (elements), batch <= 65535.
+ * Products with 64 or more rows on one side and K >= 8 run on the tensor cores
+ * (tcgen05 MMAs in TF32 with a three-way split that keeps FP32 accuracy); the
+ * others on a SIMT kernel. */
 int fw_fno_sgemm(int transA, int transB, int M, int N, int K, float alpha, const float* A, long long lda,
                  long long strideA, const float* B, long long ldb, long long strideB, float beta, float* C,
                  long long ldc, long long strideC, int batch, void* stream);
+/* Synchronous read of the FNO status word (0 or FW_FNO_TIMEOUT); clear != 0 resets it. */
+int fw_fno_status(int* status_out, int clear);
 /* Per-mode complex channel mixing, [B][C][2][K] layouts (real block, imaginary block):
  * mode 0: out = sum_i X[b][i] Y[i][o]; mode 1: out[b][i] = sum_o X[b][o] conj(Y[i][o]);
  * mode 2: out[i][o] = sum_b conj(X[b][i]) Y[b][o]. */
