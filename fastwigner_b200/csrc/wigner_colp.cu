@@ -9,9 +9,8 @@
 // and keeps the next item's data in flight while it computes the current one:
 //
 //   * the state tile (N rows x 2*CP columns) arrives in shared memory by
-//     bulk-tensor copies (TMA) issued once the current tile has been read
-//     into registers and transformed, so the copy overlaps the mid-point and
-//     the inverse transform;
+//     bulk-tensor copies (TMA) issued as soon as the current tile has been
+//     read into registers, so the copy overlaps the whole transform pair;
 //   * the phase-table tile ((N/2+1) rows x CP column pairs) arrives the same
 //     way after the current item's mid-point has read its own; consecutive
 //     items of a CTA share the column tile (work items are column-tile major),
@@ -242,14 +241,17 @@ __global__ void __launch_bounds__(CP* T, MINB)
       const float2 w = *reinterpret_cast<const float2*>(Ws + (size_t)(j + m * T) * L::WROWB + 2 * c);
       v[m] = mk<C>(w.x * s, w.y * s);
     }
-    // ---- forward transform along p; its exchange barriers also order every
-    // thread's reads of the state buffer before the next copy into it
-    fft<N, T, RV, -1, C, EXT>(v, j, ex, tw);
-    if (abort_flag) break;  // written before the transform's barriers: the same on every thread
+    // release the buffer at once, so the next copy overlaps the whole transform
+    // pair (issuing it after the forward transform, one barrier fewer, measured
+    // 0.341 vs 0.315 ms per 64 x 1024^2 launch)
+    __syncthreads();
+    if (abort_flag) break;
     if (it + 1 < last) {
       if (tid == 0) issue_w(it + 1);
       w_pending = true;
     }
+    // ---- forward transform along p
+    fft<N, T, RV, -1, C, EXT>(v, j, ex, tw);
     // ---- mid-point: wait for this item's table tile if one is in flight
     if (t_pending) {
       const bool ok_t = mbar_wait_bounded(&bars[1], ph_t, kTmaMaxPolls);

@@ -3,6 +3,7 @@ gains: wall time to a thermal state with and without the surrogate seed.
 
     python -m fastwigner_b200.surrogate [--runs 200] [--epochs 10] [--train-grid 256] [--out results.json]
     torchrun --nproc-per-node N -m fastwigner_b200.surrogate --dp ...   # data-parallel training
+    python -m fastwigner_b200.surrogate --time-network [--reps 5]          # network timings only
 
 The workload is the Morse-oscillator thermal-state problem
 (V = D (1 - exp(-a (x - x_e)))^2, D ~ U(2, 10), a ~ U(0.5, 1.5),
@@ -96,6 +97,33 @@ def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256
                 train_grid=train_grid, width=width, refine_fraction=refine_fraction, results=results)
 
 
+def time_network(grid=512, train_grid=256, n=16, reps=5, width=32, seed=0):
+    """CUDA-event times (ms, mean of `reps` after one warm-up) of the
+    surrogate's inference for `n` instances on the full grid and of one
+    training step (forward, backward, Adam) on a batch of `n` at the training
+    grid, with random weights and inputs."""
+    setup = MorseBlochSetup(grid=grid)
+    net = FNO2d(n_params=3, width=width, modes=(16, 16), layers=4, proj=128, seed=seed)
+    sur = BlochSurrogate(setup, net, train_grid=train_grid)
+    rng = np.random.default_rng(seed)
+    Ds, As = rng.uniform(2.0, 10.0, n), rng.uniform(0.5, 1.5, n)
+    X = rng.uniform(-1.0, 1.0, size=(n, 3))
+    T = torch.zeros((n, train_grid, train_grid), dtype=torch.float32, device=net.device)
+
+    def train_step():
+        _, dY = net.loss_and_grad(X, sur.xs_t, sur.ps_t, T)
+        net.backward(dY)
+        net.adam_step(1e-4)
+
+    out = {}
+    for name, fn in ((f"predict_{n}x{grid}_ms", lambda: sur.predict(Ds, As, 4.0)),
+                     (f"train_step_{n}x{train_grid}_ms", train_step)):
+        fn()
+        _, ms = timed(lambda: [fn() for _ in range(reps)])
+        out[name] = ms / reps
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--runs", type=int, default=200)
@@ -111,7 +139,13 @@ def main():
     ap.add_argument("--out", default=None)
     ap.add_argument("--dp", action="store_true",
                     help="data-parallel training, one process per GPU under torchrun (NCCL gradient all-reduce)")
+    ap.add_argument("--time-network", action="store_true",
+                    help="only time the network's inference and one training step (random weights), then exit")
+    ap.add_argument("--reps", type=int, default=5)
     a = ap.parse_args()
+    if a.time_network:
+        print(json.dumps(time_network(train_grid=a.train_grid, reps=a.reps, width=a.width)))
+        return
     group = None
     if a.dp:
         import datetime
