@@ -100,11 +100,12 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) per grid point of one column-pass launch, from the
-# ncu capture summarised in profiles/col_pass_f32_1024.md (dram__bytes_read.sum
-# + dram__bytes_write.sum of a 40-instance 1024 x 1024 launch / its points);
-# the line's roofline.traffic scales it to the points of one bench launch.
-NCU_COL_DRAM_BYTES_PER_POINT = 6.887
+# DRAM bytes (read + write) per grid point of one column-pass launch, from an
+# ncu capture of the persistent column pass (dram__bytes_read.sum +
+# dram__bytes_write.sum of a 40-instance 1024 x 1024 launch: 175.5 + 137.9 MB,
+# over its points); the line's roofline.traffic scales it to the points of one
+# bench launch.
+NCU_COL_DRAM_BYTES_PER_POINT = 7.47
 
 
 def parity_check(sim, W0, steps=20):
@@ -307,8 +308,8 @@ def run_ours(args):
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": NCU_COL_DRAM_BYTES_PER_POINT * pts,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per point of a column-pass "
-                                  "launch (profiles/col_pass_f32_1024.md), times the points of one launch",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per point of a 40-instance "
+                                  "column-pass launch (captured separately), times the points of one launch",
                 "kernel": dom_kind, "kernel_ms": dom_ms, "col_ms": col_ms, "row_ms": row_ms,
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
                 "frac_of_nominal_8000_gbs": achieved / 8000.0}
