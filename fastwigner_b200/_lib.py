@@ -93,6 +93,11 @@ _SIGNATURES = [
     ("fw_batch_set_spin_limit", c_int, [c_vp, c_ll]),
     ("fw_fno_sgemm", c_int, [c_int, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_ll, c_ll, c_vp, c_ll, c_ll,
                               ctypes.c_float, c_vp, c_ll, c_ll, c_int, c_vp]),
+    ("fw_fno_sgemm_ex", c_int, [c_int, c_int, c_int, c_int, c_int, ctypes.c_float, c_vp, c_ll, c_ll, c_vp, c_ll, c_ll,
+                                ctypes.c_float, c_vp, c_ll, c_ll, c_int, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
+    ("fw_fno_wgrad_work", c_int, [c_int, c_int, c_ll, c_int, ctypes.POINTER(c_ll)]),
+    ("fw_fno_wgrad", c_int, [c_int, c_int, c_ll, c_vp, c_ll, c_vp, c_ll, c_int, c_vp, c_ll, c_vp, c_int, c_vp]),
+    ("fw_fno_project", c_int, [c_int, c_int, c_ll, c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_ll, c_vp]),
     ("fw_fno_status", c_int, [ctypes.POINTER(c_int), c_int]),
     ("fw_fno_mix", c_int, [c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
     ("fw_fno_bias_act", c_int, [c_ll, c_int, c_ll, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),

@@ -2,75 +2,17 @@
 //
 // The FNO is small (width 32, 16 x 16 retained modes); its dense contractions --
 // truncated DFTs written as products with DFT matrices, the pointwise channel
-// maps, the projection -- all go through one batched SGEMM with optional
-// transposes.  The per-mode complex channel mixing of the spectral
+// maps, the projection, the weight gradients -- run on the tensor-core GEMM
+// (fno_umma.cu).  The per-mode complex channel mixing of the spectral
 // convolution, bias + GELU, channel reductions, the relative-L2 loss and the
-// Adam update have their own element-wise kernels.  FP32 throughout, FP64
+// Adam update have their own element-wise kernels here.  FP32 throughout, FP64
 // accumulation in the reductions.
 #include <cuda_runtime.h>
 #include <math.h>
+#include "fno_act.cuh"
 #include "fw_internal.h"
 
 namespace fw {
-
-// C[b] = alpha * op(A[b]) * op(B[b]) + beta * C[b]; op(A) is M x K, op(B) K x N,
-// row-major with leading dimensions lda, ldb, ldc; batch strides sA, sB, sC.
-constexpr int GT = 64, GK = 16;
-__global__ void __launch_bounds__(256) sgemm_kernel(int ta, int tb, int M, int N, int K, float alpha,
-                                                    const float* __restrict__ A, long long lda, long long sA,
-                                                    const float* __restrict__ B, long long ldb, long long sB,
-                                                    float beta, float* __restrict__ C, long long ldc, long long sC) {
-  __shared__ float As[GK][GT + 4];
-  __shared__ float Bs[GK][GT + 4];
-  const int bz = blockIdx.z;
-  A += (size_t)bz * sA;
-  B += (size_t)bz * sB;
-  C += (size_t)bz * sC;
-  const int row0 = blockIdx.y * GT, col0 = blockIdx.x * GT;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  float acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += GK) {
-    // load op(A)[row0..row0+63][k0..k0+15] and op(B)[k0..k0+15][col0..col0+63]
-    for (int e = threadIdx.x; e < GT * GK; e += 256) {
-      const int r = e / GK, kk = e % GK;  // A tile element (r, kk)
-      const int gr = row0 + r, gk = k0 + kk;
-      float va = 0.f;
-      if (gr < M && gk < K) va = ta ? A[(size_t)gk * lda + gr] : A[(size_t)gr * lda + gk];
-      As[kk][r] = va;
-      const int kb = e / GT, c = e % GT;  // B tile element (kb, c)
-      const int gkb = k0 + kb, gc = col0 + c;
-      float vb = 0.f;
-      if (gkb < K && gc < N) vb = tb ? B[(size_t)gc * ldb + gkb] : B[(size_t)gkb * ldb + gc];
-      Bs[kb][c] = vb;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < GK; ++kk) {
-      float a[4], bb[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) bb[jj] = Bs[kk][tx * 4 + jj];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[i][jj] = fmaf(a[i], bb[jj], acc[i][jj]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = row0 + ty * 4 + i;
-    if (r >= M) continue;
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const int c = col0 + tx * 4 + jj;
-      if (c >= N) continue;
-      float* dst = C + (size_t)r * ldc + c;
-      *dst = alpha * acc[i][jj] + (beta == 0.f ? 0.f : beta * *dst);
-    }
-  }
-}
 
 // Spectral mixing.  F: [B][Cin][2][K] (real block then imaginary block of the
 // K retained modes), R: [Cin][Cout][2][K], O: [B][Cout][2][K].
@@ -126,11 +68,6 @@ __global__ void mix_bwd_w_kernel(int Bn, int Ci, int Co, int K, const float* F, 
   dR[(((size_t)i * Co + o) * 2 + 1) * K + k] = (float)im;
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_d(float x) {
-  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
-}
-
 // pre = X + bias[c]; Y = act ? gelu(pre) : pre.  X, pre, Y: [B][C][L]
 __global__ void bias_act_kernel(long long n, int C, long long L, const float* X, const float* bias, float* pre,
                                 float* Y, int act) {
@@ -146,22 +83,46 @@ __global__ void act_bwd_kernel(long long n, const float* dY, const float* pre, f
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dpre[i] = act ? dY[i] * gelu_d(pre[i]) : dY[i];
 }
-// out[c] (+)= sum_{b, l} X[b][c][l]; one block per channel, FP64 accumulation
-__global__ void channel_sum_kernel(int Bn, int C, long long L, const float* X, float* out, int accumulate) {
+// out[c] (+)= sum_{b, l} X[b][c][l]; one 1024-thread block per channel, FP64
+// accumulation, float4 loads (four in flight per thread) when L % 4 == 0 and X
+// is 16-byte aligned
+constexpr int kCsumThreads = 1024;
+__global__ void __launch_bounds__(kCsumThreads) channel_sum_kernel(int Bn, int C, long long L, const float* X,
+                                                                   float* out, int accumulate, int vec) {
   const int c = blockIdx.x;
-  double s = 0.0;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   for (int b = 0; b < Bn; ++b) {
     const float* x = X + ((size_t)b * C + c) * L;
-    for (long long l = threadIdx.x; l < L; l += blockDim.x) s += x[l];
+    if (vec) {
+      const float4* x4 = reinterpret_cast<const float4*>(x);
+      const long long n4 = L / 4;
+      long long l = threadIdx.x;
+      for (; l + 3 * kCsumThreads < n4; l += 4 * kCsumThreads) {
+        const float4 a = __ldg(x4 + l), b1 = __ldg(x4 + l + kCsumThreads), c1 = __ldg(x4 + l + 2 * kCsumThreads),
+                     d = __ldg(x4 + l + 3 * kCsumThreads);
+        s0 += (double)a.x + a.y + (double)a.z + a.w;
+        s1 += (double)b1.x + b1.y + (double)b1.z + b1.w;
+        s2 += (double)c1.x + c1.y + (double)c1.z + c1.w;
+        s3 += (double)d.x + d.y + (double)d.z + d.w;
+      }
+      for (; l < n4; l += kCsumThreads) {
+        const float4 a = __ldg(x4 + l);
+        s0 += (double)a.x + a.y + (double)a.z + a.w;
+      }
+    } else {
+      for (long long l = threadIdx.x; l < L; l += kCsumThreads) s0 += x[l];
+    }
   }
-  __shared__ double red[256];
-  red[threadIdx.x] = s;
+  double s = (s0 + s1) + (s2 + s3);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double red[kCsumThreads / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = red[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) out[c] = (float)(t + (accumulate ? (double)out[c] : 0.0));
   }
-  if (threadIdx.x == 0) out[c] = (float)(red[0] + (accumulate ? (double)out[c] : 0.0));
 }
 // loss_b = ||Y_b - T_b||^2 / ||T_b||^2; dY = 2 (Y - T) / ||T_b||^2 / B.  One block per sample.
 __global__ void rel_l2_kernel(long long L, const float* Y, const float* T, float* dY, double* loss, int Bn) {
@@ -229,26 +190,6 @@ static int grid1(long long n) {
   return (int)(b > 8192 ? 8192 : (b < 1 ? 1 : b));
 }
 
-extern "C" int fw_fno_sgemm(int transA, int transB, int M, int N, int K, float alpha, const float* A, long long lda,
-                            long long strideA, const float* B, long long ldb, long long strideB, float beta, float* C,
-                            long long ldc, long long strideC, int batch, void* stream) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return fail(FW_EINVAL, "fw_fno_sgemm: non-positive size");
-  if (A == nullptr || B == nullptr || C == nullptr) return fail(FW_EINVAL, "fw_fno_sgemm: NULL operand");
-  if (batch > 65535) return fail(FW_EINVAL, "fw_fno_sgemm: batch > 65535");
-  if (umma_gemm_eligible(M, N, K)) {  // tensor cores (tcgen05, three-way TF32 split)
-    cudaError_t e = launch_umma_gemm(transA, transB, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc,
-                                     strideC, batch, static_cast<cudaStream_t>(stream));
-    count_launch(1);
-    return e == cudaSuccess ? FW_OK : cuda_fail(e, "fw_fno_sgemm (tensor cores)");
-  }
-  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, batch);
-  sgemm_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(transA, transB, M, N, K, alpha, A, lda, strideA, B,
-                                                                     ldb, strideB, beta, C, ldc, strideC);
-  count_launch(1);
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? FW_OK : cuda_fail(e, "fw_fno_sgemm");
-}
-
 extern "C" int fw_fno_mix(int mode, int Bn, int Ci, int Co, int K, const float* X, const float* Y, float* out,
                           void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -278,7 +219,8 @@ extern "C" int fw_fno_act_bwd(long long n, const float* dY, const float* pre, fl
 
 extern "C" int fw_fno_channel_sum(int Bn, int C, long long L, const float* X, float* out, int accumulate,
                                   void* stream) {
-  channel_sum_kernel<<<C, 256, 0, static_cast<cudaStream_t>(stream)>>>(Bn, C, L, X, out, accumulate);
+  const int vec = (L % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15u) == 0);
+  channel_sum_kernel<<<C, kCsumThreads, 0, static_cast<cudaStream_t>(stream)>>>(Bn, C, L, X, out, accumulate, vec);
   count_launch(1);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FW_OK : cuda_fail(e, "fw_fno_channel_sum");

@@ -37,10 +37,6 @@ cudaError_t launch_col(const PassArgs& a, int dtype, cudaStream_t st, int* npart
 cudaError_t launch_finalize(const PassArgs& a, int dtype, cudaStream_t st);
 cudaError_t launch_pweight_dft(const double* wp, long long wp_bs, int Mp, int P, int nb, void* out, long long out_bs,
                                int dtype, cudaStream_t st);
-bool umma_gemm_eligible(int M, int N, int K);
-cudaError_t launch_umma_gemm(int ta, int tb, int M, int N, int K, float alpha, const float* A, long long lda,
-                             long long sA, const float* B, long long ldb, long long sB, float beta, float* C,
-                             long long ldc, long long sC, int batch, cudaStream_t st);
 int fno_status_read(int* out, int clear);
 bool colp_eligible(const PassArgs& a, int dtype);
 bool rowp_eligible(const PassArgs& a, int dtype);

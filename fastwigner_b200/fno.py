@@ -37,11 +37,34 @@ def _p(t, off=0):
 class _Ops:
     def __init__(self):
         self.lib = _lib.load()
+        self._work = None  # split-K slices of the weight gradients
 
     def gemm(self, ta, tb, M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, batch, alpha=1.0, beta=0.0, oA=0, oB=0,
              oC=0):
         check(self.lib.fw_fno_sgemm(ta, tb, M, N, K, alpha, _p(A, oA), lda, sA, _p(B, oB), ldb, sB, beta, _p(C, oC),
                                     ldc, sC, batch, stream_handle()), "fw_fno_sgemm")
+
+    def gemm_ex(self, ta, tb, M, N, K, A, lda, sA, B, ldb, sB, out, ldc, sC, batch, alpha=1.0, beta=0.0, C=None,
+                bias=None, pre=None, aux=None, act=0, oA=0, oB=0):
+        """out = epilogue(alpha op(A) op(B) + beta C + bias[m]); pre (if given) = the
+        pre-activation; act 0: none, 1: GELU, 2: times GELU'(aux)."""
+        opt = lambda t: _p(t) if t is not None else None
+        check(self.lib.fw_fno_sgemm_ex(ta, tb, M, N, K, alpha, _p(A, oA), lda, sA, _p(B, oB), ldb, sB, beta, opt(C),
+                                       ldc, sC, batch, opt(bias), opt(pre), opt(aux), int(act), _p(out),
+                                       stream_handle()), "fw_fno_sgemm_ex")
+
+    def wgrad(self, rows, cols, L, dY, X, batch, out):
+        """out[r][c] = sum_b sum_l dY[b][r][l] X[b][c][l] (split-K on the tensor cores)."""
+        n = ctypes.c_longlong(0)
+        check(self.lib.fw_fno_wgrad_work(rows, cols, L, batch, ctypes.byref(n)), "fw_fno_wgrad_work")
+        if self._work is None or self._work.numel() < n.value:
+            self._work = torch.empty(n.value, dtype=torch.float32, device=dY.device)
+        check(self.lib.fw_fno_wgrad(rows, cols, L, _p(dY), rows * L, _p(X), cols * L, batch, _p(self._work),
+                                    self._work.numel(), _p(out), 0, stream_handle()), "fw_fno_wgrad")
+
+    def project(self, hidden, C, L, V, batch, Q1, c1, Q2, c2, out):
+        check(self.lib.fw_fno_project(hidden, C, L, _p(V), C * L, batch, _p(Q1), _p(c1), _p(Q2), _p(c2), _p(out), L,
+                                      stream_handle()), "fw_fno_project")
 
     def mix(self, mode, B, Ci, Co, K, X, Y, out):
         check(self.lib.fw_fno_mix(mode, B, Ci, Co, K, _p(X), _p(Y), _p(out), stream_handle()), "fw_fno_mix")
@@ -138,70 +161,81 @@ class FNO2d:
         self.input_scale, self.input_shift = np.asarray(d["__in_scale__"]), np.asarray(d["__in_shift__"])
 
     def _grid(self, G0, G1):
+        """The DFT matrices of dft_matrices in the layouts the GEMMs use: the x
+        transform's cosine and sine parts side by side, CS = [Cx | Sx] (G1 x 2mx),
+        so one product gives Fx = [v Cx | v Sx] (G0 x 2mx per channel); read as a
+        2G0 x mx matrix its rows alternate cosine / sine parts, so the p transform
+        takes Dp with its columns interleaved alike and the inverse Dpi with its
+        rows interleaved; AA = [A1; A2] (2mx x G1) maps [Gc | Gs] back to x."""
         key = (G0, G1)
         if key not in self._mats:
-            mats = dft_matrices(G0, G1, self.mp, self.mx)
+            Cx, Sx, Dp, Dpi, A1, A2 = dft_matrices(G0, G1, self.mp, self.mx)
+            Dpv = np.empty_like(Dp)
+            Dpv[:, 0::2], Dpv[:, 1::2] = Dp[:, :G0], Dp[:, G0:]
+            Dpiv = np.empty_like(Dpi)
+            Dpiv[0::2], Dpiv[1::2] = Dpi[:G0], Dpi[G0:]
+            mats = (np.concatenate([Cx, Sx], axis=1), Dpv, Dpiv, np.concatenate([A1, A2], axis=0))
             self._mats[key] = [torch.tensor(m, dtype=torch.float32, device=self.device).contiguous() for m in mats]
         return self._mats[key]
 
     # -- forward ------------------------------------------------------------------
     def forward(self, params, xs, ps, cache=True):
         """params: (B, NP) raw inputs; xs (G1,), ps (G0,) coordinates (already
-        normalised to O(1)).  Returns (B, G0, G1)."""
+        normalised to O(1)).  Returns (B, G0, G1).  With cache=False (inference)
+        no activations are kept and the two-layer projection runs fused."""
         o = self.ops
         B = params.shape[0]
         G0, G1 = len(ps), len(xs)
         L = G0 * G1
         C, NP = self.C, self.NP
-        Cx, Sx, Dp, Dpi, A1, A2 = self._grid(G0, G1)
+        CS, Dpv, Dpiv, AA = self._grid(G0, G1)
+        dev = self.device
         pr = torch.tensor((np.asarray(params, dtype=np.float64) - self.input_shift) * self.input_scale,
-                          dtype=torch.float32, device=self.device).contiguous()
-        xs_t = torch.tensor(np.asarray(xs), dtype=torch.float32, device=self.device)
-        ps_t = torch.tensor(np.asarray(ps), dtype=torch.float32, device=self.device)
-        feats = torch.empty((B, NP + 2, G0, G1), dtype=torch.float32, device=self.device)
+                          dtype=torch.float32, device=dev).contiguous()
+        xs_t = torch.tensor(np.asarray(xs), dtype=torch.float32, device=dev)
+        ps_t = torch.tensor(np.asarray(ps), dtype=torch.float32, device=dev)
+        feats = torch.empty((B, NP + 2, G0, G1), dtype=torch.float32, device=dev)
         o.features(B, NP, G0, G1, pr, xs_t, ps_t, feats)
         P = self.params
-        h = torch.empty((B, C, G0, G1), dtype=torch.float32, device=self.device)
-        o.gemm(0, 0, C, L, NP + 2, P["W0"], NP + 2, 0, feats, L, (NP + 2) * L, h, L, C * L, B)
-        v = torch.empty_like(h)
-        o.bias_act(h, C, L, P["b0"], None, v, 0)
+        v = torch.empty((B, C, G0, G1), dtype=torch.float32, device=dev)
+        o.gemm_ex(0, 0, C, L, NP + 2, P["W0"], NP + 2, 0, feats, L, (NP + 2) * L, v, L, C * L, B, bias=P["b0"])
         c = {"B": B, "G0": G0, "G1": G1, "feats": feats, "v": [], "F2": [], "pre": []}
         Kp, mx, K = self.Kp, self.mx, self.K
-        Fx2 = torch.empty((B * C, 2 * G0, mx), dtype=torch.float32, device=self.device)
-        F2 = None
+        Fx = torch.empty((B * C, G0, 2 * mx), dtype=torch.float32, device=dev)
+        Gx = torch.empty_like(Fx)
         for l in range(self.layers):
-            c["v"].append(v)
-            # truncated forward DFT: x then p
-            o.gemm(0, 0, G0, mx, G1, v, G1, L, Cx, mx, 0, Fx2, mx, 2 * G0 * mx, B * C)
-            o.gemm(0, 0, G0, mx, G1, v, G1, L, Sx, mx, 0, Fx2, mx, 2 * G0 * mx, B * C, oC=G0 * mx)
-            F2 = torch.empty((B, C, 2, K), dtype=torch.float32, device=self.device)
-            o.gemm(0, 0, 2 * Kp, mx, 2 * G0, Dp, 2 * G0, 0, Fx2, mx, 2 * G0 * mx, F2, mx, 2 * K, B * C)
-            c["F2"].append(F2)
+            if cache:
+                c["v"].append(v)
+            # truncated forward DFT: x (cosine and sine parts in one product), then p
+            o.gemm(0, 0, G0, 2 * mx, G1, v, G1, L, CS, 2 * mx, 0, Fx, 2 * mx, 2 * G0 * mx, B * C)
+            F2 = torch.empty((B, C, 2, K), dtype=torch.float32, device=dev)
+            o.gemm(0, 0, 2 * Kp, mx, 2 * G0, Dpv, 2 * G0, 0, Fx, mx, 2 * G0 * mx, F2, mx, 2 * K, B * C)
+            if cache:
+                c["F2"].append(F2)
             O2 = torch.empty_like(F2)
             o.mix(0, B, C, C, K, F2, P[f"R{l}"], O2)
-            # inverse p then x (Hermitian weights), into y
-            Gx2 = torch.empty((B * C, 2 * G0, mx), dtype=torch.float32, device=self.device)
-            o.gemm(0, 0, 2 * G0, mx, 2 * Kp, Dpi, 2 * Kp, 0, O2, mx, 2 * K, Gx2, mx, 2 * G0 * mx, B * C)
-            y = torch.empty((B, C, G0, G1), dtype=torch.float32, device=self.device)
-            o.gemm(0, 0, G0, G1, mx, Gx2, mx, 2 * G0 * mx, A1, G1, 0, y, G1, L, B * C)
-            o.gemm(0, 0, G0, G1, mx, Gx2, mx, 2 * G0 * mx, A2, G1, 0, y, G1, L, B * C, beta=1.0, oA=G0 * mx)
-            # pointwise channel map
-            o.gemm(0, 0, C, L, C, P[f"W{l + 1}"], C, 0, v, L, C * L, y, L, C * L, B, beta=1.0)
+            # inverse p, then x (Hermitian weights)
+            o.gemm(0, 0, 2 * G0, mx, 2 * Kp, Dpiv, 2 * Kp, 0, O2, mx, 2 * K, Gx, mx, 2 * G0 * mx, B * C)
+            y = torch.empty((B, C, G0, G1), dtype=torch.float32, device=dev)
+            o.gemm(0, 0, G0, G1, 2 * mx, Gx, 2 * mx, 2 * G0 * mx, AA, G1, 0, y, G1, L, B * C)
+            # + pointwise channel map + bias, GELU (not after the last layer), in place
             act = l < self.layers - 1
-            pre = torch.empty_like(y)
-            vn = torch.empty_like(y)
-            o.bias_act(y, C, L, P[f"b{l + 1}"], pre, vn, act)
-            c["pre"].append(pre)
-            v = vn
+            pre = torch.empty_like(y) if cache else None
+            o.gemm_ex(0, 0, C, L, C, P[f"W{l + 1}"], C, 0, v, L, C * L, y, L, C * L, B, beta=1.0, C=y,
+                      bias=P[f"b{l + 1}"], pre=pre, act=int(act))
+            if cache:
+                c["pre"].append(pre)
+            v = y
+        out = torch.empty((B, 1, G0, G1), dtype=torch.float32, device=dev)
+        if not cache and self.proj <= 128:
+            o.project(self.proj, C, L, v, B, P["Q1"], P["c1"], P["Q2"], P["c2"], out)
+            return out.view(B, G0, G1)
         c["vL"] = v
-        h1 = torch.empty((B, self.proj, G0, G1), dtype=torch.float32, device=self.device)
-        o.gemm(0, 0, self.proj, L, C, P["Q1"], C, 0, v, L, C * L, h1, L, self.proj * L, B)
-        pre1 = torch.empty_like(h1)
-        a1 = torch.empty_like(h1)
-        o.bias_act(h1, self.proj, L, P["c1"], pre1, a1, 1)
-        out = torch.empty((B, 1, G0, G1), dtype=torch.float32, device=self.device)
-        o.gemm(0, 0, 1, L, self.proj, P["Q2"], self.proj, 0, a1, L, self.proj * L, out, L, L, B)
-        o.bias_act(out, 1, L, P["c2"], None, out, 0)
+        pre1 = torch.empty((B, self.proj, G0, G1), dtype=torch.float32, device=dev)
+        a1 = torch.empty_like(pre1)
+        o.gemm_ex(0, 0, self.proj, L, C, P["Q1"], C, 0, v, L, C * L, a1, L, self.proj * L, B, bias=P["c1"],
+                  pre=pre1, act=1)
+        o.gemm_ex(0, 0, 1, L, self.proj, P["Q2"], self.proj, 0, a1, L, self.proj * L, out, L, L, B, bias=P["c2"])
         c.update(pre1=pre1, a1=a1)
         if cache:
             self._cache = c
@@ -216,50 +250,46 @@ class FNO2d:
             t.zero_()
         B, G0, G1 = c["B"], c["G0"], c["G1"]
         L, C, NP, Kp, mx, K, PJ = G0 * G1, self.C, self.NP, self.Kp, self.mx, self.K, self.proj
-        Cx, Sx, Dp, Dpi, A1, A2 = self._grid(G0, G1)
+        CS, Dpv, Dpiv, AA = self._grid(G0, G1)
         dev = self.device
         d_out = dout.contiguous().view(B, 1, G0, G1)
         o.csum(B, 1, L, d_out, g["c2"])
-        tmp = torch.empty((B, max(PJ, C), max(C, NP + 2)), dtype=torch.float32, device=dev)
-
-        def wgrad(dY, X, rows, cols, name):  # g[name] = sum_b dY_b (rows x L) X_b^T (L x cols)
-            o.gemm(0, 1, rows, cols, L, dY, L, rows * L, X, L, cols * L, tmp, cols, rows * cols, B)
-            o.csum(B, rows * cols, 1, tmp, g[name])
-
-        wgrad(d_out, c["a1"], 1, PJ, "Q2")
+        o.wgrad(1, PJ, L, d_out, c["a1"], B, g["Q2"])
+        # da1 = GELU'(pre1) Q2^T d_out
         da1 = torch.empty((B, PJ, G0, G1), dtype=torch.float32, device=dev)
-        o.gemm(1, 0, PJ, L, 1, P["Q2"], PJ, 0, d_out, L, L, da1, L, PJ * L, B)
-        o.act_bwd(da1, c["pre1"], da1, 1)
+        o.gemm_ex(1, 0, PJ, L, 1, P["Q2"], PJ, 0, d_out, L, L, da1, L, PJ * L, B, aux=c["pre1"], act=2)
         o.csum(B, PJ, L, da1, g["c1"])
-        wgrad(da1, c["vL"], PJ, C, "Q1")
+        o.wgrad(PJ, C, L, da1, c["vL"], B, g["Q1"])
         dv = torch.empty((B, C, G0, G1), dtype=torch.float32, device=dev)
         o.gemm(1, 0, C, L, PJ, P["Q1"], C, 0, da1, L, PJ * L, dv, L, C * L, B)
         del da1
-        dGx2 = torch.empty((B * C, 2 * G0, mx), dtype=torch.float32, device=dev)
+        dGx = torch.empty((B * C, G0, 2 * mx), dtype=torch.float32, device=dev)
+        dFx = torch.empty_like(dGx)
         dO2 = torch.empty((B, C, 2, K), dtype=torch.float32, device=dev)
         dF2 = torch.empty_like(dO2)
-        dFx2 = torch.empty_like(dGx2)
+        dpre = dv  # the last layer has no GELU
         for l in reversed(range(self.layers)):
-            act = l < self.layers - 1
-            dpre = torch.empty_like(dv)
-            o.act_bwd(dv, c["pre"][l], dpre, act)
             o.csum(B, C, L, dpre, g[f"b{l + 1}"])
             vin = c["v"][l]
-            wgrad(dpre, vin, C, C, f"W{l + 1}")
-            dvin = torch.empty_like(dv)
+            o.wgrad(C, C, L, dpre, vin, B, g[f"W{l + 1}"])
+            dvin = torch.empty_like(dpre)
             o.gemm(1, 0, C, L, C, P[f"W{l + 1}"], C, 0, dpre, L, C * L, dvin, L, C * L, B)
             # spectral path
-            o.gemm(0, 1, G0, mx, G1, dpre, G1, L, A1, G1, 0, dGx2, mx, 2 * G0 * mx, B * C)
-            o.gemm(0, 1, G0, mx, G1, dpre, G1, L, A2, G1, 0, dGx2, mx, 2 * G0 * mx, B * C, oC=G0 * mx)
-            o.gemm(1, 0, 2 * Kp, mx, 2 * G0, Dpi, 2 * Kp, 0, dGx2, mx, 2 * G0 * mx, dO2, mx, 2 * K, B * C)
+            o.gemm(0, 1, G0, 2 * mx, G1, dpre, G1, L, AA, G1, 0, dGx, 2 * mx, 2 * G0 * mx, B * C)
+            o.gemm(1, 0, 2 * Kp, mx, 2 * G0, Dpiv, 2 * Kp, 0, dGx, mx, 2 * G0 * mx, dO2, mx, 2 * K, B * C)
             o.mix(1, B, C, C, K, dO2, P[f"R{l}"], dF2)
             o.mix(2, B, C, C, K, c["F2"][l], dO2, g[f"R{l}"])
-            o.gemm(1, 0, 2 * G0, mx, 2 * Kp, Dp, 2 * G0, 0, dF2, mx, 2 * K, dFx2, mx, 2 * G0 * mx, B * C)
-            o.gemm(0, 1, G0, G1, mx, dFx2, mx, 2 * G0 * mx, Cx, mx, 0, dvin, G1, L, B * C, beta=1.0)
-            o.gemm(0, 1, G0, G1, mx, dFx2, mx, 2 * G0 * mx, Sx, mx, 0, dvin, G1, L, B * C, beta=1.0, oA=G0 * mx)
-            dv = dvin
-        o.csum(B, C, L, dv, g["b0"])
-        wgrad(dv, c["feats"], C, NP + 2, "W0")
+            o.gemm(1, 0, 2 * G0, mx, 2 * Kp, Dpv, 2 * G0, 0, dF2, mx, 2 * K, dFx, mx, 2 * G0 * mx, B * C)
+            # dvin += dFx CS^T; below the first layer that is the input's gradient
+            # times GELU'(its pre-activation): the previous layer's dpre
+            if l > 0:
+                o.gemm_ex(0, 1, G0, G1, 2 * mx, dFx, 2 * mx, 2 * G0 * mx, CS, 2 * mx, 0, dvin, G1, L, B * C,
+                          beta=1.0, C=dvin, aux=c["pre"][l - 1], act=2)
+            else:
+                o.gemm(0, 1, G0, G1, 2 * mx, dFx, 2 * mx, 2 * G0 * mx, CS, 2 * mx, 0, dvin, G1, L, B * C, beta=1.0)
+            dpre = dvin
+        o.csum(B, C, L, dpre, g["b0"])
+        o.wgrad(C, NP + 2, L, dpre, c["feats"], B, g["W0"])
         return g
 
     def adam_step(self, lr, wd=0.0):

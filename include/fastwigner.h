@@ -338,13 +338,36 @@ int fw_batch_set_spin_limit(fw_batch* batch, long long polls);
 /* ------------------------------------------------------------------------ */
 
 /* C[b] = alpha op(A[b]) op(B[b]) + beta C[b]; op(A) M x K, op(B) K x N, row-major,
- * leading dimensions lda/ldb/ldc, batch strides strideA/B/C (elements), batch <= 65535.
- * Products with 64 or more rows on one side and K >= 8 run on the tensor cores
- * (tcgen05 MMAs in TF32 with a three-way split that keeps FP32 accuracy); the
- * others on a SIMT kernel. */
+ * leading dimensions lda/ldb/ldc, batch strides strideA/B/C (elements), batch <= 65535,
+ * sizes <= 2^30.  Runs on the tensor cores (tcgen05 MMAs in TF32 with a three-way split
+ * that keeps FP32 products).  Outputs up to 32 wide on the tensor core's short side
+ * (min(M, N) <= 32) sum 32-wide K chunks in registers with round-to-nearest adds; wider
+ * ones accumulate in tensor memory, whose truncating FP32 adds leave an error growing
+ * with K (about 3e-5 of max |C| at K = 4096 for random operands). */
 int fw_fno_sgemm(int transA, int transB, int M, int N, int K, float alpha, const float* A, long long lda,
                  long long strideA, const float* B, long long ldb, long long strideB, float beta, float* C,
                  long long ldc, long long strideC, int batch, void* stream);
+/* The same product with a fused epilogue: t = alpha op(A) op(B) + beta C + bias[m]
+ * (bias may be NULL; C may be NULL when beta == 0); pre = t when pre != NULL;
+ * out = t (act 0), GELU(t) (act 1) or t GELU'(aux) (act 2).  pre, aux and out share
+ * C's layout (ldc, strideC); out may be C itself. */
+int fw_fno_sgemm_ex(int transA, int transB, int M, int N, int K, float alpha, const float* A, long long lda,
+                    long long strideA, const float* B, long long ldb, long long strideB, float beta, const float* C,
+                    long long ldc, long long strideC, int batch, const float* bias, float* pre, const float* aux,
+                    int act, float* out, void* stream);
+/* Weight gradient out[r][c] (+)= sum_b sum_l dY[b][r][l] X[b][c][l] (dY: rows x L per
+ * sample, X: cols x L, batch strides strideY / strideX) as a split-K tensor-core product
+ * into `work` and an FP64 sum of the slices; fw_fno_wgrad_work gives the floats `work`
+ * must hold for these sizes. */
+int fw_fno_wgrad_work(int rows, int cols, long long L, int batch, long long* floats_out);
+int fw_fno_wgrad(int rows, int cols, long long L, const float* dY, long long strideY, const float* X,
+                 long long strideX, int batch, float* work, long long work_floats, float* out, int accumulate,
+                 void* stream);
+/* Fused two-layer pointwise projection: out[b][l] = c2[0] + sum_j Q2[j] GELU(c1[j] +
+ * sum_c Q1[j][c] V[b][c][l]) for j < hidden <= 128 (Q1: hidden x C); the hidden layer
+ * stays in tensor memory. */
+int fw_fno_project(int hidden, int C, long long L, const float* V, long long strideV, int batch, const float* Q1,
+                   const float* c1, const float* Q2, const float* c2, float* out, long long strideOut, void* stream);
 /* Synchronous read of the FNO status word (0 or FW_FNO_TIMEOUT); clear != 0 resets it. */
 int fw_fno_status(int* status_out, int clear);
 /* Per-mode complex channel mixing, [B][C][2][K] layouts (real block, imaginary block):

@@ -38,6 +38,26 @@ def test_forward_and_gradients_match_oracle():
         assert rel(g[k].double().cpu().numpy(), go[k]) < 2e-3, k
 
 
+def test_inference_path_equals_training_path():
+    """forward(cache=False) (no stored activations, the fused projection with
+    the 128-wide hidden layer kept in tensor memory) against forward(cache=True)
+    (pre-activations stored, unfused projection) and the FP64 oracle."""
+    from fastwigner_b200.fno import FNO2d
+
+    net = FNO2d(n_params=3, width=32, modes=(8, 8), layers=4, proj=128, seed=5)
+    for l in range(4):
+        net.params[f"R{l}"].mul_(20.0)
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(5, 3))
+    xs = np.linspace(-1, 1, 96, endpoint=False)
+    ps = np.linspace(-1, 1, 64, endpoint=False)
+    a = net.forward(X, xs, ps, cache=True).double().cpu().numpy()
+    b = net.forward(X, xs, ps, cache=False).double().cpu().numpy()
+    assert rel(b, a) < 1e-5
+    o = FNOOracle({k: v.double().cpu().numpy() for k, v in net.params.items()}, 3, 32, (8, 8), 4, 128)
+    assert rel(b, o.forward(X, xs, ps)) < 1e-4
+
+
 def test_training_reduces_loss():
     from fastwigner_b200.fno import FNO2d
 
