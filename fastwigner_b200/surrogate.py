@@ -21,6 +21,7 @@ import time
 import numpy as np
 import torch
 
+from .benchmarks import ClockSampler
 from .fno import BlochBatch, BlochSurrogate, FNO2d, MorseBlochSetup, generate_dataset
 
 
@@ -42,11 +43,13 @@ def local_runs(runs, world, rank):
 
 def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256, eval_betas=(5.0, 10.0, 20.0),
               n_eval=16, refine_fraction=0.15, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
-              residual=True, log=print, group=None):
+              residual=True, log=print, group=None, beta_range=(0.1, 20.0), min_refine=1.0, save=None, load=None):
     """group: a process group for data-parallel training -- each rank
     generates its share of the runs (its own seed), the network starts from
     the same seed everywhere and the gradients are averaged before every step;
-    rank 0 alone evaluates and returns the results (the others return None)."""
+    rank 0 alone evaluates and returns the results (the others return None).
+    save / load: an .npz of the trained network's parameters; with `load` the
+    data generation and training are skipped."""
     world, rank = 1, 0
     if group is not None:
         import torch.distributed as dist
@@ -54,32 +57,44 @@ def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256
         world, rank = dist.get_world_size(group), dist.get_rank(group)
     rng = np.random.default_rng(seed + 7919 * rank)
     setup = MorseBlochSetup(grid=grid)
-    betas = np.exp(np.linspace(np.log(0.1), np.log(20.0), nbeta))
-    t0 = time.time()
-    P, S = generate_dataset(setup, local_runs(runs, world, rank), betas, rng, train_grid=train_grid)
-    t_data = time.time() - t0
+    betas = np.exp(np.linspace(np.log(beta_range[0]), np.log(beta_range[1]), nbeta))
     net = FNO2d(n_params=3, width=width, modes=modes, layers=layers, proj=128, seed=seed)
     sur = BlochSurrogate(setup, net, train_grid=train_grid, residual=residual)
-    t0 = time.time()
-    losses = sur.train(P, S, epochs=epochs, batch=batch, lr=lr, rng=rng, group=group,
-                       log=(lambda ep, l: log(f"epoch {ep}: loss {l:.3e}")) if (log and rank == 0) else None)
-    torch.cuda.synchronize()
-    t_train = time.time() - t0
+    t_data = t_train = 0.0
+    losses, n_samples = [float("nan")], 0
+    if load:
+        net.load_state_dict(dict(np.load(load)))
+    else:
+        t0 = time.time()
+        P, S = generate_dataset(setup, local_runs(runs, world, rank), betas, rng, train_grid=train_grid)
+        t_data = time.time() - t0
+        n_samples = int(len(P))
+        t0 = time.time()
+        losses = sur.train(P, S, epochs=epochs, batch=batch, lr=lr, rng=rng, group=group,
+                           log=(lambda ep, l: log(f"epoch {ep}: loss {l:.3e}")) if (log and rank == 0) else None)
+        torch.cuda.synchronize()
+        t_train = time.time() - t0
+        del P, S
+        if save and rank == 0:
+            np.savez(save, **net.state_dict())
     if rank != 0:
         return None
     dxdp = setup.dX * setup.dP
     results = []
+    erng = np.random.default_rng(seed + 104729)  # held-out wells, the same whether trained here or loaded
     for beta in eval_betas:
-        Ds = rng.uniform(2.0, 10.0, size=n_eval)
-        As = rng.uniform(0.5, 1.5, size=n_eval)
+        Ds = erng.uniform(2.0, 10.0, size=n_eval)
+        As = erng.uniform(0.5, 1.5, size=n_eval)
         bb = BlochBatch(setup, Ds, As)  # exponent tables shared by both runs
         sur.predict(Ds[:1], As[:1], beta)  # warm-up (DFT matrices for the full grid)
         bb.set_uniform().run(2)
-        (Wp, n_plain), ms_plain = timed(lambda: sur.plain_gibbs(bb, beta))
-        Wp = Wp.clone()
-        (Ws, n_seed), ms_seed = timed(lambda: sur.seeded_gibbs(bb, Ds, As, beta, refine_fraction=refine_fraction))
+        with ClockSampler() as clk:
+            (Wp, n_plain), ms_plain = timed(lambda: sur.plain_gibbs(bb, beta))
+            Wp = Wp.clone()
+            (Ws, n_seed), ms_seed = timed(lambda: sur.seeded_gibbs(bb, Ds, As, beta, refine_fraction=refine_fraction,
+                                                                   min_refine=min_refine))
         err = ((Ws - Wp).abs().amax(dim=(1, 2)).double() * dxdp).cpu().numpy()
-        seed_only = sur.predict(Ds, As, beta)
+        seed_only = sur.predict(Ds, As, beta)  # the surrogate at beta itself, no refinement
         err_seed_only = ((seed_only - Wp).abs().amax(dim=(1, 2)).double() * dxdp).cpu().numpy()
         st = setup.G // train_grid  # the same error on the training points only
         err_seed_train = ((seed_only[:, ::st, ::st] - Wp[:, ::st, ::st]).abs().amax(dim=(1, 2)).double()
@@ -89,12 +104,14 @@ def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256
                             plain_ms=ms_plain, seeded_ms=ms_seed, speedup=ms_plain / ms_seed,
                             max_err=float(err.max()), median_err=float(np.median(err)),
                             surrogate_only_max_err=float(err_seed_only.max()),
-                            surrogate_only_max_err_training_points=float(err_seed_train.max())))
+                            surrogate_only_max_err_training_points=float(err_seed_train.max()),
+                            clocks=clk.summary()))
         if log:
             log(json.dumps(results[-1]))
     return dict(data_seconds=t_data, train_seconds=t_train, final_loss=float(np.mean(losses[-50:])),
-                samples=int(len(P)) * world, ranks=world, epochs=epochs, residual=residual,
-                train_grid=train_grid, width=width, refine_fraction=refine_fraction, results=results)
+                samples=n_samples * world, loaded=load, ranks=world, epochs=epochs, residual=residual,
+                train_grid=train_grid, width=width, refine_fraction=refine_fraction, min_refine=min_refine,
+                beta_range=list(beta_range), results=results)
 
 
 def time_network(grid=512, train_grid=256, n=16, reps=5, width=32, seed=0):
@@ -136,9 +153,14 @@ def main():
     ap.add_argument("--plain-target", action="store_true",
                     help="learn the thermal state itself instead of the correction to the harmonic baseline")
     ap.add_argument("--eval-betas", default="5,10,20")
+    ap.add_argument("--beta-min", type=float, default=0.1, help="smallest recorded beta of the training data")
+    ap.add_argument("--min-refine", type=float, default=1.0,
+                    help="smallest beta interval refined by plain Bloch steps after the surrogate seed")
     ap.add_argument("--out", default=None)
     ap.add_argument("--dp", action="store_true",
                     help="data-parallel training, one process per GPU under torchrun (NCCL gradient all-reduce)")
+    ap.add_argument("--save", default=None, help="write the trained network's parameters (.npz)")
+    ap.add_argument("--load", default=None, help="evaluate a saved network (no data generation or training)")
     ap.add_argument("--time-network", action="store_true",
                     help="only time the network's inference and one training step (random weights), then exit")
     ap.add_argument("--reps", type=int, default=5)
@@ -161,7 +183,8 @@ def main():
     try:
         r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine,
                       train_grid=a.train_grid, width=a.width, lr=a.lr, residual=not a.plain_target,
-                      eval_betas=tuple(float(b) for b in a.eval_betas.split(",")), group=group)
+                      eval_betas=tuple(float(b) for b in a.eval_betas.split(",")), group=group,
+                      beta_range=(a.beta_min, 20.0), min_refine=a.min_refine, save=a.save, load=a.load)
     finally:
         if group is not None:
             import torch.distributed as dist
