@@ -110,7 +110,8 @@ def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256
             log(json.dumps(results[-1]))
     return dict(data_seconds=t_data, train_seconds=t_train, final_loss=float(np.mean(losses[-50:])),
                 samples=n_samples * world, loaded=load, ranks=world, epochs=epochs, residual=residual,
-                train_grid=train_grid, width=width, refine_fraction=refine_fraction, min_refine=min_refine,
+                train_grid=train_grid, width=width, modes=list(modes), refine_fraction=refine_fraction,
+                min_refine=min_refine,
                 beta_range=list(beta_range), results=results)
 
 
@@ -149,6 +150,7 @@ def main():
     ap.add_argument("--refine", type=float, default=0.15)
     ap.add_argument("--train-grid", type=int, default=256)
     ap.add_argument("--width", type=int, default=32)
+    ap.add_argument("--modes", type=int, default=16, help="retained Fourier modes along each axis")
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--plain-target", action="store_true",
                     help="learn the thermal state itself instead of the correction to the harmonic baseline")
@@ -182,7 +184,8 @@ def main():
         group = dist.group.WORLD
     try:
         r = run_study(runs=a.runs, nbeta=a.nbeta, epochs=a.epochs, refine_fraction=a.refine,
-                      train_grid=a.train_grid, width=a.width, lr=a.lr, residual=not a.plain_target,
+                      train_grid=a.train_grid, width=a.width, modes=(a.modes, a.modes), lr=a.lr,
+                      residual=not a.plain_target,
                       eval_betas=tuple(float(b) for b in a.eval_betas.split(",")), group=group,
                       beta_range=(a.beta_min, 20.0), min_refine=a.min_refine, save=a.save, load=a.load)
     finally:
