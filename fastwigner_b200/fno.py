@@ -9,11 +9,17 @@ signs along p, non-negative along x of the real input) and mixes channels per
 mode with learned complex weights.
 
 Every operation runs in libfastwigner's own CUDA kernels (fw_fno_*): the
-truncated DFTs are products with DFT matrices (forward normalised by 1/G, so
-a trained network evaluates at any grid resolution of the same box), the
-channel maps and projection are batched SGEMMs, the spectral mixing, bias +
-GELU, reductions, loss and Adam have dedicated kernels.  Backward passes are
-written out by hand (no autograd).  The reference has no learned component.
+truncated DFTs are products with DFT matrices (forward normalised by 1/G),
+the channel maps and projection are tensor-core GEMMs, the spectral mixing,
+bias + GELU, reductions, loss and Adam have dedicated kernels.  Backward
+passes are written out by hand (no autograd).  The reference has no learned
+component.
+
+The network's coordinate features (x and p) are not periodic over the box,
+so the truncated DFT coefficients of the activations depend on the sampling
+grid: a network trained on a 256^2 subgrid differs from itself on the full
+512^2 grid by 4-5 % of its maximum.  Train on the grid the surrogate is
+evaluated on (BlochSurrogate's default).
 """
 from __future__ import annotations
 
@@ -395,14 +401,14 @@ class BlochBatch:
         return self
 
 
-def generate_dataset(setup, n_runs, betas, rng, train_grid=128, chunk_runs=64):
+def generate_dataset(setup, n_runs, betas, rng, train_grid=None, chunk_runs=64):
     """Plain Bloch trajectories from W = const for n_runs random (D, a); the
     states at every beta in `betas` (sorted) are recorded, downsampled to
     train_grid^2.  Returns params (N, 3: D, a, beta) and states (N, g, g)."""
     Ds = rng.uniform(2.0, 10.0, size=n_runs)
     As = rng.uniform(0.5, 1.5, size=n_runs)
     betas = np.sort(np.asarray(betas))
-    stride = setup.G // train_grid
+    stride = setup.G // (train_grid or setup.G)
     params, states = [], []
     for r0 in range(0, n_runs, chunk_runs):
         Dc, Ac = Ds[r0:r0 + chunk_runs], As[r0:r0 + chunk_runs]
@@ -464,8 +470,8 @@ def normalise_params(P):
 class BlochSurrogate:
     """FNO + the thermal workload: training on plain-Bloch data and seeding."""
 
-    def __init__(self, setup: MorseBlochSetup, net: FNO2d | None = None, train_grid=128, residual=True):
-        self.s, self.g = setup, int(train_grid)
+    def __init__(self, setup: MorseBlochSetup, net: FNO2d | None = None, train_grid=None, residual=True):
+        self.s, self.g = setup, int(train_grid or setup.G)
         self.net = net or FNO2d(n_params=3, width=32, modes=(16, 16), layers=4, proj=128)
         self.xs = (setup.X / setup.XA).astype(np.float32)
         self.ps = (setup.P / setup.PA).astype(np.float32)

@@ -1,13 +1,13 @@
 """Train the FNO surrogate on plain-Bloch thermal states and measure what it
 gains: wall time to a thermal state with and without the surrogate seed.
 
-    python -m fastwigner_b200.surrogate [--runs 200] [--epochs 10] [--train-grid 256] [--out results.json]
+    python -m fastwigner_b200.surrogate [--runs 1000] [--nbeta 20] [--epochs 10] [--out results.json]
     torchrun --nproc-per-node N -m fastwigner_b200.surrogate --dp ...   # data-parallel training
     python -m fastwigner_b200.surrogate --time-network [--reps 5]          # network timings only
 
 The workload is the Morse-oscillator thermal-state problem
 (V = D (1 - exp(-a (x - x_e)))^2, D ~ U(2, 10), a ~ U(0.5, 1.5),
-beta ~ logU(0.1, 20), dbeta = 1e-3, 512^2 FP32).  Error is measured with the
+training states at beta log-spaced in [2, 20], dbeta = 1e-3, 512^2 FP32).  Error is measured with the
 reference's own metric for thermal states, max |W - W_plain| dX dP
 (wigner_bloch_fftw_1d.py:165-167), against the plain Bloch run from W = const
 on the same GPU; both runs are timed with CUDA events.
@@ -41,9 +41,9 @@ def local_runs(runs, world, rank):
     return runs // world + (1 if rank < runs % world else 0)
 
 
-def run_study(runs=200, nbeta=100, epochs=10, batch=16, grid=512, train_grid=256, eval_betas=(5.0, 10.0, 20.0),
-              n_eval=16, refine_fraction=0.15, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
-              residual=True, log=print, group=None, beta_range=(0.1, 20.0), min_refine=1.0, save=None, load=None):
+def run_study(runs=1000, nbeta=20, epochs=10, batch=16, grid=512, train_grid=512, eval_betas=(5.0, 10.0, 20.0),
+              n_eval=16, refine_fraction=0.05, seed=0, width=32, modes=(16, 16), layers=4, lr=2e-3,
+              residual=True, log=print, group=None, beta_range=(2.0, 20.0), min_refine=0.25, save=None, load=None):
     """group: a process group for data-parallel training -- each rank
     generates its share of the runs (its own seed), the network starts from
     the same seed everywhere and the gradients are averaged before every step;
@@ -144,19 +144,20 @@ def time_network(grid=512, train_grid=256, n=16, reps=5, width=32, seed=0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--runs", type=int, default=200)
-    ap.add_argument("--nbeta", type=int, default=100)
+    ap.add_argument("--runs", type=int, default=1000)
+    ap.add_argument("--nbeta", type=int, default=20)
     ap.add_argument("--epochs", type=int, default=10)
-    ap.add_argument("--refine", type=float, default=0.15)
-    ap.add_argument("--train-grid", type=int, default=256)
+    ap.add_argument("--refine", type=float, default=0.05)
+    ap.add_argument("--train-grid", type=int, default=512,
+                    help="training grid (a subgrid of the 512^2 evaluation grid; the network is not resolution-invariant)")
     ap.add_argument("--width", type=int, default=32)
     ap.add_argument("--modes", type=int, default=16, help="retained Fourier modes along each axis")
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--plain-target", action="store_true",
                     help="learn the thermal state itself instead of the correction to the harmonic baseline")
     ap.add_argument("--eval-betas", default="5,10,20")
-    ap.add_argument("--beta-min", type=float, default=0.1, help="smallest recorded beta of the training data")
-    ap.add_argument("--min-refine", type=float, default=1.0,
+    ap.add_argument("--beta-min", type=float, default=2.0, help="smallest recorded beta of the training data")
+    ap.add_argument("--min-refine", type=float, default=0.25,
                     help="smallest beta interval refined by plain Bloch steps after the surrogate seed")
     ap.add_argument("--out", default=None)
     ap.add_argument("--dp", action="store_true",
