@@ -148,7 +148,7 @@ def parity_check(sim, W0, steps=20):
 # 256^2), config 2b (von Neumann complex64 1024^2), config 3 (Bloch 512^2 Morse
 # batch), config 4 (uneven persistent batch) and config 5 (strong field with
 # collisions).  Each entry is that workload's own line, trimmed.
-OTHER_WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field")
+OTHER_WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field", "fno_predict_512")
 
 
 def other_workloads():

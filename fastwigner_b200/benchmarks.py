@@ -41,7 +41,7 @@ import numpy as np
 import torch
 
 WORKLOADS = ("moyal_fp64_256", "vn_1024", "bloch_512", "batch_uneven", "strong_field", "strong_field_frames",
-             "rho_to_wigner_1024", "moyal_absorbing_1024")
+             "rho_to_wigner_1024", "moyal_absorbing_1024", "fno_predict_512")
 
 # NVML clock-event reason bits (nvmlClocksEventReason*): reported when active.
 _REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
@@ -262,6 +262,30 @@ def bloch_512(steps=2000, n=16):
     return _line("bloch_512", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 16,
                  {"grid": [setup.G, setup.G], "instances": n, "dbeta": setup.dbeta, "passes_per_step": 2,
                   "state_bytes": pts * 4, "l2_policy": "16 MiB of states, mostly L2-resident"})
+
+
+def fno_predict_512(n=16):
+    """Inference of the Bloch surrogate (4 Fourier layers, width 32, 16 x 16
+    modes, 128-wide fused projection; random weights: timing only) for n Morse
+    instances on the 512^2 grid, harmonic baseline and normalisation included.
+    Algorithmic bytes per grid point: the 32-channel activations read or
+    written 5 times per layer (forward x-DFT read, inverse x-DFT write, channel
+    map reads of the input and of the inverse DFT, its write) x 4 layers, plus
+    the lift's write and the projection's read: 22 x 128 B = 2816 B."""
+    from .fno import BlochSurrogate, FNO2d, MorseBlochSetup
+
+    setup = MorseBlochSetup()
+    net = FNO2d(n_params=3, width=32, modes=(16, 16), layers=4, proj=128, seed=0)
+    sur = BlochSurrogate(setup, net)
+    rng = np.random.default_rng(5)
+    Ds, As = rng.uniform(2, 10, n), rng.uniform(0.5, 1.5, n)
+    ms = _timed(lambda: sur.predict(Ds, As, 4.0))
+    pts = setup.G * setup.G * n
+    line = _line("fno_predict_512", pts / (ms * 1e-3), "grid-pt/s", 1, ms, "f32", 2816,
+                 {"grid": [setup.G, setup.G], "instances": n, "layers": 4, "width": 32, "modes": [16, 16],
+                  "projection": 128, "gemm": "tcgen05 TF32, three-way split", "weights": "random (timing only)"})
+    line["metric"] = "grid points per second (surrogate inference)"
+    return line
 
 
 def batch_uneven(steps=2000, n=256):
