@@ -82,14 +82,22 @@ template <int N, int T, int CP, bool PSUM_ALIAS> struct ColpLayout {
 // Mid-point of the fused column pass with the phase-table tile in shared
 // memory (Ts: row kk holds the CP column pairs' entries, complex: 4 floats per
 // pair, real: 2 floats per pair).  The same factor closes step k and opens
-// step k+1 (time-independent Hamiltonian).  Otherwise as fused_mid.
+// step k+1 (time-independent Hamiltonian).  Otherwise as fused_mid.  v holds
+// the spectrum of the unscaled tile: the input scale sc multiplies the
+// closing factor and the observable sums instead of every element.  The
+// table row min(k, N-k), its Hermitian fold and the mirrored exchange slot of
+// N-k are resolved per m at compile time (k = j + m T, j < T), with the
+// mirror slots one per-thread base minus an immediate.
 template <int N, int T, int RV, int CP, typename EX>
 __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float2 (&v)[RV], const int j, EX& ex,
-                                                 int c, const float* Ts, float2* psum, MidSums<float>& o) {
+                                                 int c, const float* Ts, float2* psum, MidSums<float>& o,
+                                                 double sc) {
   using C = float2;
+  static_assert(N == RV * T && RV % 2 == 0 && T % RV == 0 && EX::kFold && EX::kL == ilog2_c(RV),
+                "folded mirror addressing needs T a multiple of RV and a layout padded per RV");
   const C* G = reinterpret_cast<const C*>(a.wph) + (size_t)b * a.wph_bs;
   const bool obs = a.part_out != nullptr;
-  const float h = (float)(0.5 / (double)N);
+  const float hs = (float)(0.5 / (double)N * sc);
   C u[RV];
   ex_write_natural<T, RV>(ex, j, v);
   ex.sync();
@@ -98,10 +106,12 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
   o.cb = 0;
 #pragma unroll
   for (int q = 0; q < MAXO; ++q) o.sq[q] = 0;
+  const int mbase = ex.map(N - j);  // slot of N - j (virtual for j = 0); N - k is mbase - delta(m T)
 #pragma unroll
   for (int m = 0; m < RV; ++m) {
-    const int k = j + m * T;
-    const int kk = (k <= N / 2) ? k : N - k;
+    // k = j + m T: below N/2 for m < RV/2, else the table holds row N - k (conjugated, except at k = N/2)
+    constexpr int H = RV / 2;
+    const int kk = m < H ? j + m * T : N - j - m * T;
     C ea, eb;
     if (a.tab_real) {
       const float2 e = *reinterpret_cast<const float2*>(Ts + (size_t)kk * (2 * CP) + 2 * c);
@@ -111,21 +121,32 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
       const float4 e = *reinterpret_cast<const float4*>(Ts + (size_t)kk * (4 * CP) + 4 * c);
       ea = mk<C>(e.x, e.y);
       eb = mk<C>(e.z, e.w);
+      if (m == 0 || m == H) {  // k = 0 or k = N/2 when j = 0: real entries
+        if (j == 0) {
+          ea.y = 0.f;
+          eb.y = 0.f;
+        } else if (m == H) {
+          ea.y = -ea.y;
+          eb.y = -eb.y;
+        }
+      } else if (m > H) {
+        ea.y = -ea.y;
+        eb.y = -eb.y;
+      }
     }
-    ea = herm(ea, k, N);
-    eb = herm(eb, k, N);
-    const C zc = cconj(ex.read((N - k) & (N - 1)));
-    const C A = cmul(cadd(v[m], zc), ea);   // 2 x spectrum of column a at the mid-point
-    const C Bi = cmul(csub(v[m], zc), eb);  // 2i x spectrum of column b at the mid-point
+    const int ms = m == 0 ? (j == 0 ? ex.map(0) : mbase) : mbase - EX::delta(m * T);
+    const C zc = cconj(ex.read_at(ms));
+    const C A = cmul(cadd(v[m], zc), ea);   // 2/sc x spectrum of column a at the mid-point
+    const C Bi = cmul(csub(v[m], zc), eb);  // 2i/sc x spectrum of column b at the mid-point
     if (obs) {
       o.s2 += (double)(A.x * A.x + A.y * A.y + Bi.x * Bi.x + Bi.y * Bi.y);
       if (m == 0 && j == 0) {
         o.ca = A.x;
         o.cb = Bi.y;
       }
-      u[m] = mk<C>(A.x + Bi.y, A.y - Bi.x);  // 2 x (spectrum a + spectrum b)
+      u[m] = mk<C>(A.x + Bi.y, A.y - Bi.x);  // 2/sc x (spectrum a + spectrum b)
     }
-    v[m] = cscale(cadd(cmul(A, ea), cmul(Bi, eb)), h);
+    v[m] = cscale(cadd(cmul(A, ea), cmul(Bi, eb)), hs);
   }
   // per-bin sums over the tile's CP column pairs; lane c ends with bins
   // m = c * RV/CP + i
@@ -143,6 +164,13 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
       for (int q = 0; q < MAXO; ++q)
         if (q < a.Mp) o.sq[q] += (double)u.x * (double)g[q].x + (double)u.y * (double)g[q].y;
     }
+  }
+  if (obs) {  // the sums of the unscaled spectrum, scaled once
+    o.s2 *= sc * sc;
+    o.ca *= sc;
+    o.cb *= sc;
+#pragma unroll
+    for (int q = 0; q < MAXO; ++q) o.sq[q] *= sc;
   }
 }
 
@@ -234,12 +262,11 @@ __global__ void __launch_bounds__(CP* T, MINB)
     } else {
       abort_flag = 1;
     }
-    C v[RV];
-    const float s = (float)sc;
+    C v[RV];  // unscaled: the input scale is applied at the mid-point
 #pragma unroll
     for (int m = 0; m < RV; ++m) {
       const float2 w = *reinterpret_cast<const float2*>(Ws + (size_t)(j + m * T) * L::WROWB + 2 * c);
-      v[m] = mk<C>(w.x * s, w.y * s);
+      v[m] = mk<C>(w.x, w.y);
     }
     // release the buffer at once, so the next copy overlaps the whole transform
     // pair (issuing it after the forward transform, one barrier fewer, measured
@@ -265,7 +292,7 @@ __global__ void __launch_bounds__(CP* T, MINB)
       if (abort_flag) break;
     }
     MidSums<float> o;
-    fused_mid_staged<N, T, RV, CP>(a, b, v, j, ex, c, Ts, psum, o);  // ends with a CTA barrier
+    fused_mid_staged<N, T, RV, CP>(a, b, v, j, ex, c, Ts, psum, o, sc);  // ends with a CTA barrier
     const int xa = tile * 2 * CP + 2 * c;
     if (a.part_out != nullptr) mid_store<float, N, CP, NTHR>(a, b, tile, ctl.ntiles, o, xa, ored);
     // the next item's table tile (the p-weight sums in the table buffer have
