@@ -82,13 +82,15 @@ template <int N, int T, int CP, bool PSUM_ALIAS> struct ColpLayout {
 // Mid-point of the fused column pass with the phase-table tile in shared
 // memory (Ts: row kk holds the CP column pairs' entries, complex: 4 floats per
 // pair, real: 2 floats per pair).  The same factor closes step k and opens
-// step k+1 (time-independent Hamiltonian).  Otherwise as fused_mid.  v holds
+// step k+1 (time-independent Hamiltonian).  Otherwise as fused_mid.  Without
+// FUSED the pass is one potential half-step (the opening one of a call, or the
+// closing one with the observables of the result).  v holds
 // the spectrum of the unscaled tile: the input scale sc multiplies the
 // closing factor and the observable sums instead of every element.  The
 // table row min(k, N-k), its Hermitian fold and the mirrored exchange slot of
 // N-k are resolved per m at compile time (k = j + m T, j < T), with the
 // mirror slots one per-thread base minus an immediate.
-template <int N, int T, int RV, int CP, typename EX>
+template <int N, int T, int RV, int CP, bool FUSED, typename EX>
 __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float2 (&v)[RV], const int j, EX& ex,
                                                  int c, const float* Ts, float2* psum, MidSums<float>& o,
                                                  double sc) {
@@ -146,7 +148,9 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
       }
       u[m] = mk<C>(A.x + Bi.y, A.y - Bi.x);  // 2/sc x (spectrum a + spectrum b)
     }
-    v[m] = cscale(cadd(cmul(A, ea), cmul(Bi, eb)), hs);
+    // fused: close step k and open step k+1 with the same factor; a single
+    // half-step (the opening one of a call, or its closing one) repacks A, Bi
+    v[m] = FUSED ? cscale(cadd(cmul(A, ea), cmul(Bi, eb)), hs) : cscale(cadd(A, Bi), hs);
   }
   // per-bin sums over the tile's CP column pairs; lane c ends with bins
   // m = c * RV/CP + i
@@ -179,7 +183,7 @@ struct ColpCtl {
   int tab_inst;  // phase tables per instance (1) or one for the batch (0)
 };
 
-template <int N, int T, int CP, int MINB, bool BMAJOR, bool PSUM_ALIAS>
+template <int N, int T, int CP, int MINB, bool BMAJOR, bool PSUM_ALIAS, bool FUSED>
 __global__ void __launch_bounds__(CP* T, MINB)
     col_persist_kernel(const __grid_constant__ CUtensorMap mW, const __grid_constant__ CUtensorMap mT, PassArgs a,
                        ColpCtl ctl) {
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(CP* T, MINB)
       if (abort_flag) break;
     }
     MidSums<float> o;
-    fused_mid_staged<N, T, RV, CP>(a, b, v, j, ex, c, Ts, psum, o, sc);  // ends with a CTA barrier
+    fused_mid_staged<N, T, RV, CP, FUSED>(a, b, v, j, ex, c, Ts, psum, o, sc);  // ends with a CTA barrier
     const int xa = tile * 2 * CP + 2 * c;
     if (a.part_out != nullptr) mid_store<float, N, CP, NTHR>(a, b, tile, ctl.ntiles, o, xa, ored);
     // the next item's table tile (the p-weight sums in the table buffer have
@@ -371,9 +375,10 @@ cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
       !encode_3d(&mT, a.tab1, tab_cols, (uint64_t)(P / 2 + 1), (uint64_t)ntab, trow, tinst, (uint32_t)tab_rowf,
                  (uint32_t)TabBox<N>::ROWS, CU_TENSOR_MAP_L2_PROMOTION_L2_128B))
     return cudaErrorInvalidValue;
-  auto kern = col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS>;
-  static PerDeviceOnce attr;
-  cudaError_t e = set_smem_once(attr, kern, L::BYTES);
+  auto kern = a.fuse_mid ? col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, true>
+                         : col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, false>;
+  static PerDeviceOnce attr[2];
+  cudaError_t e = set_smem_once(attr[a.fuse_mid ? 1 : 0], kern, L::BYTES);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -387,14 +392,18 @@ cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
 }
 }  // namespace
 
-// The persistent column pass handles a fused FP32 column pass with one
-// time-independent table (tab1 == tab2, no separable factors, no x-p mask, no
-// blends) whose tiles and strides meet the bulk-copy rules, over enough work
+// The persistent column pass handles an FP32 column pass with one
+// time-independent table (tab1 == tab2 when fused, or a single half-step
+// without tab2; no separable factors, no x-p mask, no blends; the p-weight
+// spectra when p-observables are taken) whose tiles and strides meet the
+// bulk-copy rules, over enough work
 // items to fill the GPU at least twice; it uses the regular launch shape
 // (ColCfg) of the transform length, so the partial-sum records per instance
 // are the ones the plan sized for.
 bool colp_eligible(const PassArgs& a, int dtype) {
-  if (dtype != FW_F32 || !a.fuse_mid || a.tab1 != a.tab2 || a.g1 != nullptr || a.g2 != nullptr) return false;
+  if (dtype != FW_F32 || a.tab1 == nullptr || a.g1 != nullptr || a.g2 != nullptr) return false;
+  if (a.fuse_mid ? a.tab1 != a.tab2 : a.tab2 != nullptr) return false;
+  if (a.part_out != nullptr && a.Mp > 0 && a.wph == nullptr) return false;  // p-observables need the weight spectra
   if (a.tab_real) return false;  // Bloch tables: the regular column pass
   if (a.bxp != nullptr || a.blend_pre || a.blend_post || a.small_shape) return false;
   if (a.P != 1024) return false;
