@@ -8,8 +8,9 @@ instance.  A batch of 8 already takes every code path of the 64-instance
 bench launch: the regular launch shapes (8 x 64 column tiles >= the SM
 count), the per-instance totals kernel (batch >= 4), the vector loads of the
 shared phase table (tab_vec) and the fused mid-point column pass with its
-p-weight spectra.  Every instance is compared with the oracle restatement of
-WignerMoyalFTTW1D.propagate (wigner_moyal_fftw_1d.py:418-440).
+p-weight spectra.  A batch of 16 adds the persistent row pass.  Every instance
+is compared with the oracle restatement of WignerMoyalFTTW1D.propagate
+(wigner_moyal_fftw_1d.py:418-440).
 
 Tolerances (tests/parity_tables.py): FP64 1e-10 relative on W and every
 observable; FP32 1e-5 relative L2 of W for a short run, and for long runs
@@ -99,6 +100,21 @@ def test_bench_plan_short_run_meets_the_fixed_fp32_tolerance():
     sim, W0n, obs = _bench_plan(8, "float32", steps, seed=7)
     W = sim.W.double().cpu().numpy()
     for b in (0, 7):
+        o = _oracle(W0n[b])
+        o.propagate(steps)
+        assert _rel(W[b], o.W) < 1e-5, b
+
+
+def test_bench_plan_batch16_persistent_row_pass():
+    """A batch of 16 (16 x 512 row pairs: enough work for the persistent row
+    pass, which a batch of 8 leaves to the regular row kernel; both persistent
+    passes and the call's single half-steps then run) against the oracle over
+    20 FP32 steps at 1e-5, the first and the last instance (whose last row
+    pair ends the state buffer)."""
+    steps = 20
+    sim, W0n, obs = _bench_plan(16, "float32", steps, seed=11)
+    W = sim.W.double().cpu().numpy()
+    for b in (0, 15):
         o = _oracle(W0n[b])
         o.propagate(steps)
         assert _rel(W[b], o.W) < 1e-5, b
