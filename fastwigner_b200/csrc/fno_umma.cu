@@ -40,8 +40,9 @@
 // leaves the chip.
 //
 // Every mbarrier wait is bounded: on expiry the CTA records FW_FNO_TIMEOUT in
-// the FNO status word, writes NaN into its tile, waits once more (bounded)
-// for its MMAs, frees its TMEM and returns.
+// the FNO status word, writes NaN into the tile it was computing (its later
+// tiles are left unwritten), waits once more (bounded) for its MMAs, frees its
+// TMEM and returns.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>

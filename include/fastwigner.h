@@ -46,7 +46,7 @@ extern "C" {
 /* device status words: of a batched launch (fw_batch_status) and of a plan (fw_wigner_plan_status) */
 #define FW_BATCH_TIMEOUT 1  /* a grid barrier gave up waiting; the launch returned early */
 #define FW_PASS_TIMEOUT 2   /* a pass's bulk copy into shared memory did not complete; its CTA returned early */
-#define FW_FNO_TIMEOUT 3    /* a tensor-core GEMM of the FNO gave up waiting for its MMAs; its tile holds NaN */
+#define FW_FNO_TIMEOUT 3    /* a tensor-core GEMM of the FNO gave up waiting for its MMAs; its output is invalid (NaN where it stopped) */
 
 /* step structure of fw_wigner_propagate */
 #define FW_STEP_FUSED 0 /* V/2 K V/2 with the closing V/2 of step n fused with the
