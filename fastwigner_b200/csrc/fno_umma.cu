@@ -54,14 +54,7 @@ namespace fw {
 
 __device__ int g_fno_status;  // FW_FNO_TIMEOUT when a tensor-core GEMM gave up waiting
 
-namespace {
-
-constexpr int UM = 128;  // tile rows (tensor-core M)
-constexpr int UK = 32;   // K per shared-memory chunk (four MMAs of K = 8)
-constexpr long long kUmmaMaxPolls = 1LL << 20;
-
-enum { EPI_NONE = 0, EPI_GELU = 1, EPI_DGELU = 2 };
-
+// arguments of one tensor-core GEMM launch
 struct UmmaArgs {
   int urows, vrows, K;  // D = U V^T is urows x vrows; contraction length K
   int ksplit, kchunk;   // CTA z = b ksplit + s contracts k in [s kchunk, min(K, (s + 1) kchunk))
@@ -82,6 +75,15 @@ struct UmmaArgs {
   const float* dotb;
   int uvec, vvec;  // K-contiguous operand with 16-byte aligned rows: float4 loads
 };
+
+namespace umma {  // named (external linkage): host helpers take lambdas over these types
+
+constexpr int UM = 128;  // tile rows (tensor-core M)
+constexpr int UK = 32;   // K per shared-memory chunk (four MMAs of K = 8)
+constexpr long long kUmmaMaxPolls = 1LL << 20;
+
+enum { EPI_NONE = 0, EPI_GELU = 1, EPI_DGELU = 2 };
+
 
 // canonical K-major no-swizzle offset (floats) of the 4-float row (r, k-group
 // g) of a tile with `rows` rows: core matrix (r/8, g) of 8 x 4 floats
@@ -602,7 +604,7 @@ int check_gemm_args(long long M, long long N, long long K, int batch, const void
   if (batch > 65535) return fail(FW_EINVAL, w + ": batch > 65535");
   return FW_OK;
 }
-}  // namespace
+}  // namespace umma
 
 int fno_status_read(int* out, int clear) {
   cudaError_t e = cudaMemcpyFromSymbol(out, g_fno_status, sizeof(int));
@@ -616,6 +618,7 @@ int fno_status_read(int* out, int clear) {
 }  // namespace fw
 
 using namespace fw;
+using namespace fw::umma;
 
 extern "C" int fw_fno_sgemm(int transA, int transB, int M, int N, int K, float alpha, const float* A, long long lda,
                             long long strideA, const float* B, long long ldb, long long strideB, float beta, float* C,
