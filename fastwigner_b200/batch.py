@@ -229,7 +229,9 @@ class WignerMoyalUnevenBatch:
         X = (ctypes.c_int * n)(*[int(s["X_gridDIM"]) for s in self.specs])
         self._h = _lib.c_vp()
         check(self._lib.fw_batch_create(n, P, X, 0, ctypes.byref(self._h)), "fw_batch_create")
-        self.W, self._tabs, self.dXdP = [], [], []
+        self.GROUPED = self._lib.fw_batch_num_variants()  # the variant index of the grouped mode
+        self._groups = self._make_groups()
+        self.W, self._tabs, self.dXdP = [None] * n, [None] * n, [None] * n
         for i, s in enumerate(self.specs):
             Pn, Xn = int(s["P_gridDIM"]), int(s["X_gridDIM"])
             dX, dP = 2.0 * s["X_amplitude"] / Xn, 2.0 * s["P_amplitude"] / Pn
@@ -242,19 +244,59 @@ class WignerMoyalUnevenBatch:
                                  (Pn // 2 + 1, Xn))
             ek = np.broadcast_to(np.exp(-1j * self.dt / h * (s["K"](p + 0.5 * h * la) - s["K"](p - 0.5 * h * la))),
                                  (Pn, Xn // 2 + 1))
-            tv = torch.view_as_real(to_device(ev, torch.complex64, self.device)).contiguous()
-            tk = torch.view_as_real(to_device(ek, torch.complex64, self.device)).contiguous()
-            W = torch.zeros((Pn, Xn), dtype=torch.float32, device=self.device)
-            self.W.append(W)
-            self._tabs.append((tv, tk))
-            self.dXdP.append(dX * dP)
+            # the instance's state and tables are slices of its shape group's
+            # buffers, which the grouped mode propagates as one plan
+            g, k = self._slot[i]
+            W = g["W"][k]
+            tv, tk = g["tab"][2 * k], g["tab"][2 * k + 1]
+            tv[: ev.size].copy_(to_device(np.ascontiguousarray(ev).ravel(), torch.complex64, self.device))
+            tk[: ek.size].copy_(to_device(np.ascontiguousarray(ek).ravel(), torch.complex64, self.device))
+            self.W[i] = W
+            self._tabs[i] = (tv, tk)
+            self.dXdP[i] = dX * dP
             s.update(X=x, P=p, dX=dX, dP=dP)
             check(self._lib.fw_batch_set_instance(self._h, i, ptr(W), ptr(tv), ptr(tk), dX * dP),
                   "fw_batch_set_instance")
+        self._graph = None
+        self._graph_key = None
         self.variant = 0
         if variant is None:
             variant = self.autotune(autotune_steps)
         self.set_variant(variant)
+
+    def _make_groups(self):
+        """Instances of equal (P, X, dX dP), in order of first appearance: one
+        state buffer (n x P x X), one table buffer (2n slots of S complex
+        entries, V table then K table per instance, S the larger table rounded
+        to an even count so every slot starts on 16 bytes) and one plan each."""
+        from ._lib import FW_F32
+
+        keys, members = [], {}
+        for i, s in enumerate(self.specs):
+            Pn, Xn = int(s["P_gridDIM"]), int(s["X_gridDIM"])
+            dxdp = (2.0 * s["X_amplitude"] / Xn) * (2.0 * s["P_amplitude"] / Pn)
+            key = (Pn, Xn, dxdp)
+            if key not in members:
+                keys.append(key)
+                members[key] = []
+            members[key].append(i)
+        groups, self._slot = [], {}
+        for key in keys:
+            Pn, Xn, dxdp = key
+            idx = members[key]
+            S = max((Pn // 2 + 1) * Xn, Pn * (Xn // 2 + 1))
+            S += S % 2
+            g = {"P": Pn, "X": Xn, "dxdp": dxdp, "idx": idx, "S": S,
+                 "idx_t": torch.tensor(idx, dtype=torch.long, device=self.device),
+                 "W": torch.zeros((len(idx), Pn, Xn), dtype=torch.float32, device=self.device),
+                 "tab": torch.zeros((2 * len(idx), S), dtype=torch.complex64, device=self.device),
+                 "plan": _lib.c_vp()}
+            check(self._lib.fw_wigner_plan_create(Pn, Xn, len(idx), FW_F32, ctypes.byref(g["plan"])),
+                  "fw_wigner_plan_create")
+            for k, i in enumerate(idx):
+                self._slot[i] = (g, k)
+            groups.append(g)
+        return groups
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -264,9 +306,24 @@ class WignerMoyalUnevenBatch:
             except Exception:
                 pass
             self._h = None
+        self._graph = None
+        for g in getattr(self, "_groups", []):
+            if g["plan"].value:
+                try:
+                    self._lib.fw_wigner_plan_destroy(g["plan"])
+                except Exception:
+                    pass
+                g["plan"].value = None
 
     def set_variant(self, v):
-        check(self._lib.fw_batch_set_variant(self._h, int(v)), "fw_batch_set_variant")
+        """0, 1: launch shapes of the persistent cooperative kernel; GROUPED:
+        one plan per shape group (the regular and persistent pass kernels of
+        the single-shape path, all groups replayed as one CUDA graph)."""
+        if not 0 <= int(v) <= self.GROUPED:
+            raise ValueError(f"variant must be in [0, {self.GROUPED}]")
+        if int(v) != self.GROUPED:
+            check(self._lib.fw_batch_set_variant(self._h, int(v)), "fw_batch_set_variant")
+            self._graph = self._graph_key = self._graph_obs = None
         self.variant = int(v)
 
     def set_wignerfunctions(self, states):
@@ -281,14 +338,67 @@ class WignerMoyalUnevenBatch:
         (steps x ninst x 2: sum W, sum W^2)."""
         if obs is None:
             obs = torch.empty((steps, len(self.specs), 2), dtype=torch.float64, device=self.device)
-        check(self._lib.fw_batch_propagate(self._h, int(steps), ptr(obs), 1 if use_graph else 0, stream_handle()),
-              "fw_batch_propagate")
+        if self.variant == self.GROUPED:
+            self._propagate_grouped(int(steps), use_graph, obs)
+        else:
+            check(self._lib.fw_batch_propagate(self._h, int(steps), ptr(obs), 1 if use_graph else 0,
+                                               stream_handle()), "fw_batch_propagate")
         self.t += steps * self.dt
         return obs
 
+    def _launch_groups(self, steps, obs, obs_g):
+        from ._lib import FW_STEP_FUSED
+
+        # the groups one after another on the current stream: replayed from a
+        # graph, the small groups' launches are short enough that side streams
+        # gained nothing over this order (0.669 vs 0.668 ms per step for the
+        # 256-instance mix of 16 shapes) and a multi-stream graph lost 17 %
+        for g, og in zip(self._groups, obs_g):
+            d = WignerDesc()
+            d.W = ptr(g["W"])
+            d.w_bstride = g["P"] * g["X"]
+            d.step_kind = FW_STEP_FUSED
+            d.tabV, d.tabK = ptr(g["tab"][0]), ptr(g["tab"][1])
+            d.tab_bstride = 2 * g["S"]
+            d.obs_out = ptr(og)
+            d.dxdp = g["dxdp"]
+            d.in_scale = 1.0
+            check(self._lib.fw_wigner_propagate(g["plan"], ctypes.byref(d), steps, stream_handle()),
+                  "fw_wigner_propagate")
+        for g, og in zip(self._groups, obs_g):
+            obs.index_copy_(1, g["idx_t"], og)
+
+    def _propagate_grouped(self, steps, use_graph, obs):
+        if not use_graph:
+            obs_g = [torch.empty((steps, len(g["idx"]), 2), dtype=torch.float64, device=self.device)
+                     for g in self._groups]
+            self._launch_groups(steps, obs, obs_g)
+            return
+        key = (steps, obs.data_ptr())
+        if self._graph_key != key:
+            self._graph = None
+            obs_g = [torch.empty((steps, len(g["idx"]), 2), dtype=torch.float64, device=self.device)
+                     for g in self._groups]
+            self._launch_groups(steps, obs, obs_g)  # first call direct: one-time set-up outside the capture
+            torch.cuda.synchronize(self.device)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                self._launch_groups(steps, obs, obs_g)
+            self._graph, self._graph_key, self._graph_obs = graph, key, obs_g
+            # the direct call above already advanced the states by `steps`
+            return
+        self._graph.replay()
+
     def status(self):
+        """The persistent kernel's device status word (FW_BATCH_TIMEOUT after an
+        expired grid barrier), or else the first non-zero status of the
+        grouped mode's plans."""
         st = ctypes.c_int()
         check(self._lib.fw_batch_status(self._h, ctypes.byref(st)), "fw_batch_status")
+        for g in self._groups:
+            if st.value:
+                break
+            check(self._lib.fw_wigner_plan_status(g["plan"], ctypes.byref(st), 0), "fw_wigner_plan_status")
         return st.value
 
     def set_status(self, value=0):
@@ -329,20 +439,24 @@ class WignerMoyalUnevenBatch:
                     return int(table[key]["variant"])
             except (ValueError, KeyError, OSError):
                 pass
-        saved = [W.clone() for W in self.W]
+        saved = [g["W"].clone() for g in self._groups]
         t_saved = self.t
         times = {}
-        for v in range(self._lib.fw_batch_num_variants()):
+        obs = torch.empty((steps, len(self.specs), 2), dtype=torch.float64, device=self.device)
+        for v in range(self.GROUPED + 1):
+            # each mode as propagate(use_graph=True) runs it: the first call
+            # captures the graph, the second replays it
             self.set_variant(v)
-            self.propagate(2, use_graph=False)  # warm-up
+            self.propagate(steps, use_graph=True, obs=obs)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            self.propagate(steps, use_graph=False)
+            self.propagate(steps, use_graph=True, obs=obs)
             e1.record()
             torch.cuda.synchronize()
             times[v] = e0.elapsed_time(e1) / steps
-        for W, s in zip(self.W, saved):
-            W.copy_(s)
+        self._graph = self._graph_key = self._graph_obs = None
+        for g, s in zip(self._groups, saved):
+            g["W"].copy_(s)
         self.t = t_saved
         best = min(times, key=times.get)
         if cache:

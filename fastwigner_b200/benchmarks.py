@@ -19,9 +19,10 @@ seeds follow the workloads the propagators are specified on:
   dbeta = 1e-3, 16 instances with their own exponent tables.
 * ``batch_uneven`` -- 256 independent FP32 Moyal instances, grids drawn per
   axis from {128, 256, 512, 1024}, double wells a x^4 - b x^2 with
-  a ~ U(0.02, 0.1), b ~ U(0.5, 2), amplitude 10, dt 0.005, one persistent
-  cooperative launch per call replayed as a CUDA graph (launch shape from the
-  autotuner).
+  a ~ U(0.02, 0.1), b ~ U(0.5, 2), amplitude 10, dt 0.005, replayed as a
+  CUDA graph; the autotuner picks between the launch shapes of the persistent
+  cooperative kernel (one launch per call) and the grouped mode (one plan per
+  grid shape, the groups one after another in one graph).
 * ``strong_field`` -- velocity-gauge laser-driven soft-core atom with
   random-collision dephasing: V0 = -1/sqrt(x^2 + 1), E(t) = E0 sin^2(pi t/T)
   sin(w t), E0 ~ U(0.01, 0.1), w = 0.057, T = 8 cycles, x: 2048 points
@@ -310,7 +311,8 @@ def batch_uneven(steps=2000, n=256):
     pts = sum(s["P_gridDIM"] * s["X_gridDIM"] for s in specs)
     return _line("batch_uneven", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 16,
                  {"instances": n, "grids_per_axis": list(sizes), "total_points": pts, "state_bytes": pts * 4,
-                  "variant": sim.variant, "graph": True, "passes_per_step": 2,
+                  "variant": sim.variant, "variants": {"persistent": list(range(sim.GROUPED)), "grouped": sim.GROUPED},
+                  "autotune_ms_per_step": getattr(sim, "autotune_ms", None), "graph": True, "passes_per_step": 2,
                   "l2_policy": f"{pts * 4 / 2**20:.0f} MiB of states, above L2"},
                  {"status": sim.status()})
 

@@ -34,13 +34,14 @@ def initial(s, rng):
     return (np.exp(-(s["X"] - x0) ** 2 / 0.25 - 0.25 * (s["P"] - p0) ** 2) + 0 * s["X"] * s["P"]).astype(np.float32)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, "grouped"])
 def test_uneven_batch_matches_oracle(variant):
     from fastwigner_b200.batch import WignerMoyalUnevenBatch
 
     rng = np.random.default_rng(3)
     specs = make_specs(rng)
-    b = WignerMoyalUnevenBatch(specs, dt=0.005, variant=variant)
+    b = WignerMoyalUnevenBatch(specs, dt=0.005, variant=0)
+    b.set_variant(b.GROUPED if variant == "grouped" else variant)
     states = [initial(s, rng) for s in b.specs]
     b.set_wignerfunctions(states)
     obs = b.propagate(25, use_graph=False)
@@ -72,6 +73,52 @@ def test_graph_replay_equals_direct_launch_and_autotune_cache(tmp_path, monkeypa
         b.propagate(10, use_graph=False)
     for Wa, Wb in zip(a.W, b.W):  # same work per item whichever CTA takes it: bit-identical
         assert np.array_equal(Wa.cpu().numpy(), Wb.cpu().numpy())
+
+
+def test_grouped_mode_equals_persistent_kernel_on_shared_shapes():
+    """Instances of one shape and box share a plan in the grouped mode: six
+    1024^2 instances (enough column pairs for the persistent pass kernels),
+    three 256 x 512 and two 128^2, interleaved, each with its own potential.
+    The grouped mode (graph replay after a direct first call) agrees with the
+    persistent cooperative kernel and, for one instance per shape, with the
+    oracle; graph replays equal direct launches bit for bit."""
+    from fastwigner_b200.batch import WignerMoyalUnevenBatch
+
+    rng = np.random.default_rng(9)
+    shapes = [(1024, 1024), (256, 512), (1024, 1024), (128, 128), (1024, 1024), (256, 512),
+              (1024, 1024), (128, 128), (1024, 1024), (256, 512), (1024, 1024)]
+    specs = []
+    for P, X in shapes:
+        V, K = dw(rng.uniform(0.02, 0.1), rng.uniform(0.5, 2.0))
+        specs.append(dict(P_gridDIM=P, X_gridDIM=X, X_amplitude=8.0, P_amplitude=7.0, V=V, K=K))
+    a = WignerMoyalUnevenBatch(specs, dt=0.005, variant=0)
+    b = WignerMoyalUnevenBatch(specs, dt=0.005, variant=0)
+    c = WignerMoyalUnevenBatch(specs, dt=0.005, variant=0)
+    b.set_variant(b.GROUPED)
+    c.set_variant(c.GROUPED)
+    assert len(b._groups) == 3
+    states = [initial(s, rng) for s in a.specs]
+    for x in (a, b, c):
+        x.set_wignerfunctions(states)
+    import torch
+
+    ob = torch.empty((10, len(specs), 2), dtype=torch.float64, device="cuda")
+    for _ in range(3):  # b: a direct call that captures the graph, then two replays
+        oa = a.propagate(10, use_graph=False)
+        b.propagate(10, use_graph=True, obs=ob)
+        c.propagate(10, use_graph=False)
+    assert a.status() == 0 and b.status() == 0 and c.status() == 0
+    for Wa, Wb, Wc in zip(a.W, b.W, c.W):
+        assert rel(Wb.double().cpu().numpy(), Wa.double().cpu().numpy()) < 1e-5
+        assert np.array_equal(Wb.cpu().numpy(), Wc.cpu().numpy())
+    np.testing.assert_allclose(b.purity(ob), a.purity(oa), rtol=1e-5)
+    for i in (0, 1, 3):
+        s = a.specs[i]
+        o = WignerOracle(X_gridDIM=s["X_gridDIM"], X_amplitude=8.0, P_gridDIM=s["P_gridDIM"], P_amplitude=7.0,
+                         dt=0.005, V=s["V"], K=s["K"])
+        o.set_wignerfunction(states[i].astype(np.float64))
+        o.propagate(30)
+        assert rel(b.W[i].double().cpu().numpy(), o.W) < 1e-5
 
 
 @pytest.mark.parametrize("B", [3, 12])
