@@ -209,15 +209,23 @@ def _autotune_path():
 
 class WignerMoyalUnevenBatch:
     """Independent FP32 Moyal instances with their own grids (P, X in
-    {128, 256, 512, 1024}), amplitudes and Hamiltonians, advanced by one
-    persistent cooperative launch per ``propagate`` call (optionally replayed
-    as a CUDA graph).  Conventions are WignerMoyalFTTW1D's (static
-    Hamiltonians; exponents as in wigner_moyal_fftw_1d.py:164-213).
+    {128, 256, 512, 1024}), amplitudes and Hamiltonians.  Conventions are
+    WignerMoyalFTTW1D's (static Hamiltonians; exponents as in
+    wigner_moyal_fftw_1d.py:164-213).  Two execution modes, both optionally
+    replayed as a CUDA graph:
+
+    * variants 0 .. GROUPED-1: one persistent cooperative launch per
+      ``propagate`` call over every instance, in one of the launch shapes;
+    * GROUPED: instances of one (P, X, dX dP) share one state buffer, one
+      table buffer and one plan of the single-shape path, and the groups run
+      one after another (the persistent pass kernels where a group is large
+      enough, the regular ones otherwise).
 
     ``specs``: one dict per instance with X_gridDIM, P_gridDIM, X_amplitude,
     P_amplitude, V (callable of x), K (callable of p).  ``variant`` None picks
-    the launch shape with the autotuner (timings cached in a JSON file keyed by
-    GPU and size mix, the analogue of FFTW wisdom)."""
+    the mode with the autotuner (timings cached in a JSON file keyed by GPU
+    and size mix, the analogue of FFTW wisdom).  ``W[i]`` is instance i's
+    state (a view into its group's buffer, shared by both modes)."""
 
     def __init__(self, specs, *, dt, t=0.0, hbar=1.0, variant=None, autotune_steps=10):
         self.dt, self.t, self.hbar = float(dt), float(t), float(hbar)
