@@ -238,12 +238,14 @@ extern "C" int fw_wigner_propagate(fw_wigner_plan* plan, const fw_wigner_desc* d
   auto ring = [&](int k) { return plan->ring + (size_t)(k & 1) * ring_slot; };
   auto hist = [&](int k) { return d->obs_out == nullptr ? nullptr : d->obs_out + (size_t)k * B * M; };
 
-  // With a totals buffer and a batch of 4 or more, a small kernel after each
-  // column pass with partial sums reduces them per instance (and records the
-  // observable history); the next pass reads one total per instance.  For
-  // smaller batches (where that launch would cost more than it saves) and for
-  // fixed-scratch plans every CTA of the next pass reduces the partials itself.
-  const bool totals = plan->tot != nullptr && B >= 4;
+  // With a totals buffer, a batch of 4 or more and more than 8 partial records
+  // per instance, a small kernel after each column pass with partial sums
+  // reduces them per instance (and records the observable history); the next
+  // pass reads one total per instance.  For smaller batches or few records
+  // (where that launch costs more than it saves: about 1 us per step for
+  // 14-18 instances of 256 x 128 ... 512 x 256) and for fixed-scratch plans
+  // every CTA of the next pass reduces the partials itself.
+  const bool totals = plan->tot != nullptr && B >= 4 && plan->nparts > 8;
   auto col = [&](PassArgs a) -> int {
     a.tw = plan->twP;
     int np = 0;
