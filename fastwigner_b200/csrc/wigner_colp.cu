@@ -80,17 +80,19 @@ template <int N, int T, int CP, bool PSUM_ALIAS> struct ColpLayout {
 };
 
 // Mid-point of the fused column pass with the phase-table tile in shared
-// memory (Ts: row kk holds the CP column pairs' entries, complex: 4 floats per
-// pair, real: 2 floats per pair).  The same factor closes step k and opens
-// step k+1 (time-independent Hamiltonian).  Otherwise as fused_mid.  Without
-// FUSED the pass is one potential half-step (the opening one of a call, or the
-// closing one with the observables of the result).  v holds
+// memory (Ts: row kk holds the CP column pairs' complex entries, 4 floats per
+// pair; real Bloch tables take the regular column pass).  The same factor
+// closes step k and opens step k+1 (time-independent Hamiltonian).  Otherwise
+// as fused_mid.  Without FUSED the pass is one potential half-step (the
+// opening one of a call, or the closing one with the observables of the
+// result).  OBS: the observable sums are taken (a compile-time switch, like
+// the table kind: 0.3127 -> 0.3045 ms per 64 x 1024^2 launch).  v holds
 // the spectrum of the unscaled tile: the input scale sc multiplies the
 // closing factor and the observable sums instead of every element.  The
 // table row min(k, N-k), its Hermitian fold and the mirrored exchange slot of
 // N-k are resolved per m at compile time (k = j + m T, j < T), with the
 // mirror slots one per-thread base minus an immediate.
-template <int N, int T, int RV, int CP, bool FUSED, typename EX>
+template <int N, int T, int RV, int CP, bool FUSED, bool OBS, typename EX>
 __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float2 (&v)[RV], const int j, EX& ex,
                                                  int c, const float* Ts, float2* psum, MidSums<float>& o,
                                                  double sc) {
@@ -98,7 +100,7 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
   static_assert(N == RV * T && RV % 2 == 0 && T % RV == 0 && EX::kFold && EX::kL == ilog2_c(RV),
                 "folded mirror addressing needs T a multiple of RV and a layout padded per RV");
   const C* G = reinterpret_cast<const C*>(a.wph) + (size_t)b * a.wph_bs;
-  const bool obs = a.part_out != nullptr;
+  constexpr bool obs = OBS;
   const float hs = (float)(0.5 / (double)N * sc);
   C u[RV];
   ex_write_natural<T, RV>(ex, j, v);
@@ -115,11 +117,7 @@ __device__ __forceinline__ void fused_mid_staged(const PassArgs& a, int b, float
     constexpr int H = RV / 2;
     const int kk = m < H ? j + m * T : N - j - m * T;
     C ea, eb;
-    if (a.tab_real) {
-      const float2 e = *reinterpret_cast<const float2*>(Ts + (size_t)kk * (2 * CP) + 2 * c);
-      ea = mk<C>(e.x, 0.f);
-      eb = mk<C>(e.y, 0.f);
-    } else {
+    {
       const float4 e = *reinterpret_cast<const float4*>(Ts + (size_t)kk * (4 * CP) + 4 * c);
       ea = mk<C>(e.x, e.y);
       eb = mk<C>(e.z, e.w);
@@ -183,7 +181,7 @@ struct ColpCtl {
   int tab_inst;  // phase tables per instance (1) or one for the batch (0)
 };
 
-template <int N, int T, int CP, int MINB, bool BMAJOR, bool PSUM_ALIAS, bool FUSED>
+template <int N, int T, int CP, int MINB, bool BMAJOR, bool PSUM_ALIAS, bool FUSED, bool OBS>
 __global__ void __launch_bounds__(CP* T, MINB)
     col_persist_kernel(const __grid_constant__ CUtensorMap mW, const __grid_constant__ CUtensorMap mT, PassArgs a,
                        ColpCtl ctl) {
@@ -210,7 +208,7 @@ __global__ void __launch_bounds__(CP* T, MINB)
   const int last = (int)((long long)(blockIdx.x + 1) * n_items / gridDim.x);
   if (first >= last) return;  // the same for every thread of the CTA
   const int tid = threadIdx.x;
-  const int tab_rowf = (a.tab_real ? 2 : 4) * CP;  // floats per table-tile row
+  constexpr int tab_rowf = 4 * CP;  // floats per table-tile row (complex tables)
   const uint32_t w_bytes = (uint32_t)(L::W_FLOATS * 4);
   const uint32_t t_bytes = (uint32_t)(TabBox<N>::NL * TabBox<N>::ROWS * tab_rowf * 4);
   auto item_t = [&](int it) { return BMAJOR ? it % ctl.ntiles : it / a.batch; };
@@ -296,13 +294,13 @@ __global__ void __launch_bounds__(CP* T, MINB)
       if (abort_flag) break;
     }
     MidSums<float> o;
-    fused_mid_staged<N, T, RV, CP, FUSED>(a, b, v, j, ex, c, Ts, psum, o, sc);  // ends with a CTA barrier
+    fused_mid_staged<N, T, RV, CP, FUSED, OBS>(a, b, v, j, ex, c, Ts, psum, o, sc);  // ends with a CTA barrier
     const int xa = tile * 2 * CP + 2 * c;
-    if (a.part_out != nullptr) mid_store<float, N, CP, NTHR>(a, b, tile, ctl.ntiles, o, xa, ored);
+    if (OBS) mid_store<float, N, CP, NTHR>(a, b, tile, ctl.ntiles, o, xa, ored);
     // the next item's table tile (the p-weight sums in the table buffer have
     // been read before mid_store's barrier)
     t_pending = it + 1 < last && tab_key(it + 1) != tab_key(it);
-    if (PSUM_ALIAS && a.part_out == nullptr) __syncthreads();  // no mid_store barrier to lean on
+    if (PSUM_ALIAS && !OBS) __syncthreads();  // no mid_store barrier to lean on
     if (tid == 0 && t_pending) issue_t(it + 1);
     // ---- inverse transform and store
     fft<N, T, RV, +1, C, EXT>(v, j, ex, tw);
@@ -375,10 +373,13 @@ cudaError_t launch_colp_cfg(const PassArgs& a, cudaStream_t st, int* nparts) {
       !encode_3d(&mT, a.tab1, tab_cols, (uint64_t)(P / 2 + 1), (uint64_t)ntab, trow, tinst, (uint32_t)tab_rowf,
                  (uint32_t)TabBox<N>::ROWS, CU_TENSOR_MAP_L2_PROMOTION_L2_128B))
     return cudaErrorInvalidValue;
-  auto kern = a.fuse_mid ? col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, true>
-                         : col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, false>;
-  static PerDeviceOnce attr[2];
-  cudaError_t e = set_smem_once(attr[a.fuse_mid ? 1 : 0], kern, L::BYTES);
+  const bool obs = a.part_out != nullptr;
+  auto kern = a.fuse_mid ? (obs ? col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, true, true>
+                                : col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, true, false>)
+                         : (obs ? col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, false, true>
+                                : col_persist_kernel<N, T, CP, S::MINB, S::BMAJOR, S::PSUM_ALIAS, false, false>);
+  static PerDeviceOnce attr[4];
+  cudaError_t e = set_smem_once(attr[(a.fuse_mid ? 2 : 0) + (obs ? 1 : 0)], kern, L::BYTES);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
