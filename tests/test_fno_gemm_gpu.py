@@ -117,6 +117,30 @@ def test_fused_epilogue(act, M, N, K):
     assert np.abs(f(out) - ref).max() / np.abs(ref).max() < 1e-5
 
 
+def test_gelu_pointwise_accuracy():
+    """The epilogue's GELU and GELU' against the exact functions on a dense
+    grid of FP32 arguments in [-12, 12]: within 3e-7 max(1, |x|) (FP32 rounding
+    of the result alone is 0.6e-7 |x|).  The GEMM term is zero (K = 1, zero
+    operands), so out = act(C)."""
+    import torch
+
+    from fastwigner_b200 import _lib
+
+    lib = _lib.load()
+    M, N = 512, 1024
+    x = np.linspace(-12.0, 12.0, M * N).astype(np.float32).reshape(1, M, N)
+    xt, ones = _t(x), _t(np.ones_like(x))
+    zA, zB = _t(np.zeros((1, M, 1))), _t(np.zeros((1, 1, N)))
+    xd = x.astype(np.float64)
+    for act, cin, aux, ref in ((1, xt, None, _gelu(xd)), (2, ones, xt, _gelu_d(xd))):
+        out = torch.empty_like(xt)
+        _lib.check(lib.fw_fno_sgemm_ex(0, 0, M, N, 1, 1.0, _p(zA), 1, M, _p(zB), N, N, 1.0, _p(cin), N, M * N, 1,
+                                       None, None, _p(aux) if aux is not None else None, act, _p(out), None))
+        torch.cuda.synchronize()
+        err = np.abs(out.double().cpu().numpy() - ref) / np.maximum(1.0, np.abs(xd))
+        assert err.max() < 3e-7, (act, err.max())
+
+
 @pytest.mark.parametrize("rows,cols,L,batch", [(32, 32, 65536, 16), (128, 32, 4096, 3), (1, 128, 10000, 4),
                                                (32, 5, 1000, 2), (7, 3, 37, 5)])
 def test_split_k_weight_gradient(rows, cols, L, batch):
