@@ -144,6 +144,40 @@ def parity_check(sim, W0, steps=20):
             "against": "FP64 oracle (numpy restatement of WignerMoyalFTTW1D.propagate)", "tol_rel_l2": 1e-5}
 
 
+def uneven_parity(sim, steps=5):
+    """Outside the timed region: the uneven batch (in the mode the autotuner
+    picked) advances `steps` more steps from its current states; its smallest
+    and largest instances are compared with the FP64 oracle (the checker,
+    oracle/wigner_oracle.py) run from the same states."""
+    import torch
+
+    from oracle.wigner_oracle import WignerOracle
+
+    sizes = [s["P_gridDIM"] * s["X_gridDIM"] for s in sim.specs]
+    insts = sorted({int(np.argmin(sizes)), int(np.argmax(sizes))})
+    W0 = [sim.W[i].double().cpu().numpy() for i in insts]
+    t0 = sim.t
+    sim.propagate(steps, use_graph=False)
+    torch.cuda.synchronize()
+    rel = 0.0
+    for i, w0 in zip(insts, W0):
+        s = sim.specs[i]
+        o = WignerOracle(X_gridDIM=s["X_gridDIM"], X_amplitude=s["X_amplitude"], P_gridDIM=s["P_gridDIM"],
+                         P_amplitude=s["P_amplitude"], dt=sim.dt, V=s["V"], K=s["K"], t=t0,
+                         fft_workers=os.cpu_count())
+        o.set_wignerfunction(w0)
+        o.propagate(steps)
+        W = sim.W[i].double().cpu().numpy()
+        rel = max(rel, float(np.linalg.norm(W - o.W) / np.linalg.norm(o.W)))
+    return {"rel_l2": rel, "steps": steps, "instances": insts,
+            "grids": [[sim.specs[i]["P_gridDIM"], sim.specs[i]["X_gridDIM"]] for i in insts],
+            "mode": sim.variant, "status": sim.status(),
+            "against": "FP64 oracle from the batch's own states after the timed calls", "tol_rel_l2": 1e-5}
+
+
+WORKLOAD_CHECKS = {"batch_uneven": uneven_parity}
+
+
 # The other configurations (fastwigner_b200/benchmarks.py), measured after the
 # headline on the same GPU so that every run records them: config 1 (FP64 Moyal
 # 256^2), config 2b (von Neumann complex64 1024^2), config 3 (Bloch 512^2 Morse
@@ -158,11 +192,14 @@ def other_workloads():
     out = {}
     for name in OTHER_WORKLOADS:
         try:
-            line = benchmarks.run(name)
+            kw = {"check": WORKLOAD_CHECKS[name]} if name in WORKLOAD_CHECKS else {}
+            line = benchmarks.run(name, **kw)
             out[name] = {"value": line["value"], "unit": line["unit"], "ms_per_step": line["ms_per_step"],
                          "dtype": line["dtype"], "roofline_frac": line["roofline"]["frac"],
                          "algorithmic_bytes_per_unit": line["roofline"]["algorithmic_bytes_per_unit"],
                          "clocks_sm_mhz": line["clocks"].get("sm_mhz"), "config": line["config"]}
+            if "parity" in line:
+                out[name]["parity"] = line["parity"]
         except Exception as e:  # a failing side workload must not cost the headline line
             out[name] = {"error": f"{type(e).__name__}: {e}"}
     return out
@@ -406,7 +443,8 @@ def main():
 
         if args.workload not in benchmarks.WORKLOADS:
             ap.error(f"unknown workload {args.workload}")
-        print(json.dumps(benchmarks.run(args.workload)), flush=True)
+        kw = {"check": WORKLOAD_CHECKS[args.workload]} if args.workload in WORKLOAD_CHECKS else {}
+        print(json.dumps(benchmarks.run(args.workload, **kw)), flush=True)
         return 0
     return run_ours(args)
 

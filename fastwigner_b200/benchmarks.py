@@ -289,7 +289,9 @@ def fno_predict_512(n=16):
     return line
 
 
-def batch_uneven(steps=2000, n=256):
+def batch_uneven(steps=2000, n=256, check=None):
+    """``check``: optional callable given the batch after the timed calls
+    (outside the timing); what it returns goes into the line as ``parity``."""
     from .batch import WignerMoyalUnevenBatch
 
     rng = np.random.default_rng(11)
@@ -309,12 +311,15 @@ def batch_uneven(steps=2000, n=256):
     obs = torch.empty((steps, n, 2), dtype=torch.float64, device="cuda")
     ms = _timed(lambda: sim.propagate(steps, use_graph=True, obs=obs))
     pts = sum(s["P_gridDIM"] * s["X_gridDIM"] for s in specs)
+    extra = {"status": sim.status()}
+    if check is not None:
+        extra["parity"] = check(sim)
     return _line("batch_uneven", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 16,
                  {"instances": n, "grids_per_axis": list(sizes), "total_points": pts, "state_bytes": pts * 4,
                   "variant": sim.variant, "variants": {"persistent": list(range(sim.GROUPED)), "grouped": sim.GROUPED},
                   "autotune_ms_per_step": getattr(sim, "autotune_ms", None), "graph": True, "passes_per_step": 2,
                   "l2_policy": f"{pts * 4 / 2**20:.0f} MiB of states, above L2"},
-                 {"status": sim.status()})
+                 extra)
 
 
 def _strong_field_sim():
