@@ -175,7 +175,32 @@ def uneven_parity(sim, steps=5):
             "against": "FP64 oracle from the batch's own states after the timed calls", "tol_rel_l2": 1e-5}
 
 
-WORKLOAD_CHECKS = {"batch_uneven": uneven_parity}
+def fp64_256_parity(sim, kw, steps=5):
+    """Outside the timed region: the FP64 256^2 batch advances `steps` more
+    steps from its current states; its first and last instances are compared
+    with the FP64 oracle run from the same states (tolerance 1e-10)."""
+    import torch
+
+    from oracle.wigner_oracle import WignerOracle
+
+    insts = sorted({0, sim.batch - 1})
+    W0 = [sim.W[b].cpu().numpy() for b in insts]
+    t0 = sim.t
+    sim.propagate(steps)
+    torch.cuda.synchronize()
+    rel = 0.0
+    for b, w0 in zip(insts, W0):
+        o = WignerOracle(X_gridDIM=kw["X_gridDIM"], X_amplitude=kw["X_amplitude"], P_gridDIM=kw["P_gridDIM"],
+                         P_amplitude=kw["P_amplitude"], dt=kw["dt"], V=kw["V"], K=kw["K"], t=t0,
+                         fft_workers=os.cpu_count())
+        o.set_wignerfunction(w0)
+        o.propagate(steps)
+        rel = max(rel, float(np.linalg.norm(sim.W[b].cpu().numpy() - o.W) / np.linalg.norm(o.W)))
+    return {"rel_l2": rel, "steps": steps, "instances": insts,
+            "against": "FP64 oracle from the batch's own states after the timed calls", "tol_rel_l2": 1e-10}
+
+
+WORKLOAD_CHECKS = {"batch_uneven": uneven_parity, "moyal_fp64_256": fp64_256_parity}
 
 
 # The other configurations (fastwigner_b200/benchmarks.py), measured after the

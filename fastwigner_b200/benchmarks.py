@@ -210,7 +210,10 @@ def _line(name, value, unit, steps, ms, dtype, bytes_per_unit, config, extra=Non
 
 
 # ---------------------------------------------------------------------------
-def moyal_fp64_256(steps=1000, big_batch=512):
+def moyal_fp64_256(steps=1000, big_batch=512, check=None):
+    """``check``: optional callable given the big batch after its timed calls
+    and the constructor keywords (outside the timing); its result goes into
+    the line as ``parity``."""
     from .batch import WignerMoyalBatch
 
     kw = dict(X_gridDIM=256, X_amplitude=8.0, P_gridDIM=256, P_amplitude=7.0, dt=0.01,
@@ -224,13 +227,18 @@ def moyal_fp64_256(steps=1000, big_batch=512):
         obs = torch.empty((steps, B, 8), dtype=torch.float64, device="cuda")
         ms = _timed(lambda: sim.propagate(steps, obs=obs))
         res[B] = (256 * 256 * B * steps / (ms * 1e-3), ms)
+        if B == big_batch and check is not None:
+            res["parity"] = check(sim, kw)
         del sim
     v, ms = res[big_batch]
+    extra = {"single_instance": {"value": res[1][0], "ms_per_step": res[1][1] / steps,
+                                 "note": "512 KiB state, L2-resident"}}
+    if "parity" in res:
+        extra["parity"] = res["parity"]
     return _line("moyal_fp64_256", v, "grid-pt*steps/s", steps, ms, "f64", 32,
                  {"grid": [256, 256], "amplitudes": [8.0, 7.0], "dt": 0.01, "batch": big_batch,
                   "passes_per_step": 2, "l2_policy": f"batch of {big_batch} copies (256 MiB) streams from HBM"},
-                 {"single_instance": {"value": res[1][0], "ms_per_step": res[1][1] / steps,
-                                      "note": "512 KiB state, L2-resident"}})
+                 extra)
 
 
 def vn_1024(steps=400):
