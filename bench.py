@@ -200,7 +200,26 @@ def fp64_256_parity(sim, kw, steps=5):
             "against": "FP64 oracle from the batch's own states after the timed calls", "tol_rel_l2": 1e-10}
 
 
-WORKLOAD_CHECKS = {"batch_uneven": uneven_parity, "moyal_fp64_256": fp64_256_parity}
+def vn_1024_parity(q, steps=5):
+    """Outside the timed region: the complex64 von Neumann propagator of the
+    vn_1024 workload (double well 0.05 x^4 - x^2, K = p^2/2) advances `steps`
+    more steps from its current density matrix; compared with the FP64 density-
+    matrix oracle (oracle/rho_oracle.py) run from the same matrix."""
+    from oracle.rho_oracle import RhoOracle
+
+    R0 = q.rho.get().astype(np.complex128)
+    t0 = q.t
+    R = q.propagate(steps).get()
+    o = RhoOracle(X_gridDIM=1024, X_amplitude=10.0, dt=0.005, t=t0, V=lambda x: 0.05 * x ** 4 - x ** 2,
+                  K=lambda p: 0.5 * p * p)
+    o.set_rho(R0)
+    o.propagate(steps)
+    return {"rel_l2": float(np.linalg.norm(R - o.rho) / np.linalg.norm(o.rho)), "steps": steps,
+            "against": "FP64 density-matrix oracle from the propagator's own state after the timed calls",
+            "tol_rel_l2": 1e-5}
+
+
+WORKLOAD_CHECKS = {"batch_uneven": uneven_parity, "moyal_fp64_256": fp64_256_parity, "vn_1024": vn_1024_parity}
 
 
 # The other configurations (fastwigner_b200/benchmarks.py), measured after the

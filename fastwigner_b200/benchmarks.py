@@ -241,7 +241,9 @@ def moyal_fp64_256(steps=1000, big_batch=512, check=None):
                  extra)
 
 
-def vn_1024(steps=400):
+def vn_1024(steps=400, check=None):
+    """``check``: optional callable given the propagator after its timed calls
+    (outside the timing); its result goes into the line as ``parity``."""
     from .rho import RhoVNeumannCUDA1D
 
     q = RhoVNeumannCUDA1D(X_gridDIM=1024, X_amplitude=10.0, dt=0.005, t=0.0, K="0.5 * P * P",
@@ -256,7 +258,8 @@ def vn_1024(steps=400):
     n = 1024 * 1024
     return _line("vn_1024", n * steps / (ms * 1e-3), "matrix-el*steps/s", steps, ms, "c64", 32,
                  {"grid": [1024, 1024], "amplitude": 10.0, "dt": 0.005, "passes_per_step": 2,
-                  "observables_per_step": 5, "l2_policy": "8 MiB state, L2-resident (effective figure)"})
+                  "observables_per_step": 5, "l2_policy": "8 MiB state, L2-resident (effective figure)"},
+                 {"parity": check(q)} if check is not None else None)
 
 
 def bloch_512(steps=2000, n=16):
