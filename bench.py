@@ -219,7 +219,35 @@ def vn_1024_parity(q, steps=5):
             "tol_rel_l2": 1e-5}
 
 
-WORKLOAD_CHECKS = {"batch_uneven": uneven_parity, "moyal_fp64_256": fp64_256_parity, "vn_1024": vn_1024_parity}
+def bloch_512_parity(bb, setup, Ds, As, steps=5):
+    """Outside the timed region: the Morse Bloch batch advances `steps` more
+    imaginary-time steps from its current states; its first and last instances
+    are compared with the FP64 oracle's CUDA-convention Bloch step
+    (wigner_bloch_cuda_1d.py:229-254) run from the same states."""
+    import torch
+
+    from oracle.wigner_oracle import WignerOracle
+
+    insts = sorted({0, bb.n - 1})
+    W0 = [bb.W[i].double().cpu().numpy() for i in insts]
+    bb.run(steps)
+    torch.cuda.synchronize()
+    rel = 0.0
+    for i, w0 in zip(insts, W0):
+        o = WignerOracle(X_gridDIM=setup.G, X_amplitude=setup.XA, P_gridDIM=setup.G, P_amplitude=setup.PA,
+                         dt=setup.dbeta, V=setup.V(Ds[i], As[i]), K=lambda p: 0.5 * p * p, fft_workers=os.cpu_count())
+        o.setup_bloch_cuda()
+        o.set_wignerfunction(w0)
+        for _ in range(steps):
+            o.bloch_single_step(setup.dbeta)
+        rel = max(rel, float(np.linalg.norm(bb.W[i].double().cpu().numpy() - o.W) / np.linalg.norm(o.W)))
+    return {"rel_l2": rel, "steps": steps, "instances": insts,
+            "against": "FP64 oracle (CUDA-convention Bloch step) from the batch's own states after the timed calls",
+            "tol_rel_l2": 1e-5}
+
+
+WORKLOAD_CHECKS = {"batch_uneven": uneven_parity, "moyal_fp64_256": fp64_256_parity, "vn_1024": vn_1024_parity,
+                   "bloch_512": bloch_512_parity}
 
 
 # The other configurations (fastwigner_b200/benchmarks.py), measured after the

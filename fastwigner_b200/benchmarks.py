@@ -262,7 +262,10 @@ def vn_1024(steps=400, check=None):
                  {"parity": check(q)} if check is not None else None)
 
 
-def bloch_512(steps=2000, n=16):
+def bloch_512(steps=2000, n=16, check=None):
+    """``check``: optional callable given the batch, the setup and the Morse
+    parameters after the timed calls (outside the timing); its result goes
+    into the line as ``parity``."""
     from .fno import BlochBatch, MorseBlochSetup
 
     rng = np.random.default_rng(3)
@@ -273,7 +276,8 @@ def bloch_512(steps=2000, n=16):
     pts = setup.G * setup.G * n
     return _line("bloch_512", pts * steps / (ms * 1e-3), "grid-pt*steps/s", steps, ms, "f32", 16,
                  {"grid": [setup.G, setup.G], "instances": n, "dbeta": setup.dbeta, "passes_per_step": 2,
-                  "state_bytes": pts * 4, "l2_policy": "16 MiB of states, mostly L2-resident"})
+                  "state_bytes": pts * 4, "l2_policy": "16 MiB of states, mostly L2-resident"},
+                 {"parity": check(bb, setup, Ds, As)} if check is not None else None)
 
 
 def fno_predict_512(n=16):
