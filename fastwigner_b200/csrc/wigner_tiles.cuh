@@ -312,18 +312,34 @@ template <typename Rl, int N, int CP, int NTHR>
 __device__ __forceinline__ void mid_store(const PassArgs& a, int b, int tile, int ntiles, MidSums<Rl>& o, int xa,
                                           double (*ored)[2 + 2 * MAXO]) {
   static_assert(CP <= 32, "DC lanes must sit in warp 0");
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    o.s2 += __shfl_xor_sync(0xffffffffu, o.s2, off);
-#pragma unroll
-    for (int q = 0; q < MAXO; ++q)
-      if (q < a.Mp) o.sq[q] += __shfl_xor_sync(0xffffffffu, o.sq[q], off);
-  }
+  static_assert(MAXO == 4, "the paired reduction below takes s2 and three bin sums");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) {
-    ored[warp][1] = o.s2 * (0.25 / (double)N);
+  {
+    // s2 and the first three bin sums (zero beyond Mp) reduce together: at
+    // each of the first two levels a lane keeps half of its values and sends
+    // the other half, so the four cost 2 + 1 + 3 shuffles instead of 4 x 5.
+    // Lane 8 v ends with the warp's total of value v (s2, sq0, sq1, sq2).
+    // (Persistent column pass: 0.3047 -> 0.2888 ms per 64 x 1024^2 launch.)
+    const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0;
+    double k0 = h16 ? o.sq[1] : o.s2, k1 = h16 ? o.sq[2] : o.sq[0];
+    const double s0 = h16 ? o.s2 : o.sq[1], s1 = h16 ? o.sq[0] : o.sq[2];
+    k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+    k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+    double k = h8 ? k1 : k0;
+    k += __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8);
 #pragma unroll
-    for (int q = 0; q < MAXO; ++q) ored[warp][2 + MAXO + q] = o.sq[q] * (0.5 / (double)N);
+    for (int off = 4; off > 0; off >>= 1) k += __shfl_xor_sync(0xffffffffu, k, off);
+    if ((lane & 7) == 0) {
+      const int v = lane >> 3;
+      if (v == 0) ored[warp][1] = k * (0.25 / (double)N);
+      else ored[warp][2 + MAXO + v - 1] = k * (0.5 / (double)N);
+    }
+    if (a.Mp > 3) {
+      double k3 = o.sq[3];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) k3 += __shfl_xor_sync(0xffffffffu, k3, off);
+      if (lane == 0) ored[warp][2 + MAXO + 3] = k3 * (0.5 / (double)N);
+    }
   }
   if (warp == 0) {
     const double da = 0.5 * o.ca, db = 0.5 * o.cb;
