@@ -249,6 +249,10 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
   o.cb = 0;
 #pragma unroll
   for (int q = 0; q < MAXO; ++q) o.sq[q] = 0;
+  // bins per block of the paired per-bin reduction (at most CP)
+  constexpr int PB = CP >= 4 ? 4 : (CP >= 2 ? 2 : 1);
+  static_assert(RV % PB == 0, "bin blocks must tile the thread's bins");
+  C ub[PB];
 #pragma unroll
   for (int m = 0; m < RV; ++m) {
     const int k = j + m * T;
@@ -277,14 +281,39 @@ __device__ __forceinline__ void fused_mid(const PassArgs& a, int b, cplx_t<Rl> (
       }
       if (a.Mp > 0) {
         // 2 x (spectrum a + spectrum b), summed over the tile's CP column pairs
-        // (lanes c of one row group are adjacent); one lane per bin stores it
-        Rl ur = A.x + Bi.y, ui = A.y - Bi.x;
+        // (lanes c of one row group are adjacent) for a block of PB bins at a
+        // time: the first log2(PB) shuffle levels scatter the block (a lane
+        // keeps half of its values and sends the other half), the rest sum one
+        // value, and one lane per bin stores it (FP64 256^2, batch 512: 0.5266 ->
+        // 0.5070 ms per step against a full butterfly per bin)
+        ub[m % PB] = mk<C>(A.x + Bi.y, A.y - Bi.x);
+        if (m % PB == PB - 1) {
+          C kp = ub[0];
+          int vi = 0;
+          if constexpr (PB == 4) {
+            const bool up = (c & (CP / 2)) != 0, up2 = (c & (CP / 4)) != 0;
+            C k0 = up ? ub[2] : ub[0], k1 = up ? ub[3] : ub[1];
+            const C s0 = up ? ub[0] : ub[2], s1 = up ? ub[1] : ub[3];
+            k0 = cadd(k0, mk<C>(__shfl_xor_sync(0xffffffffu, s0.x, CP / 2), __shfl_xor_sync(0xffffffffu, s0.y, CP / 2)));
+            k1 = cadd(k1, mk<C>(__shfl_xor_sync(0xffffffffu, s1.x, CP / 2), __shfl_xor_sync(0xffffffffu, s1.y, CP / 2)));
+            kp = up2 ? k1 : k0;
+            const C s = up2 ? k0 : k1;
+            kp = cadd(kp, mk<C>(__shfl_xor_sync(0xffffffffu, s.x, CP / 4), __shfl_xor_sync(0xffffffffu, s.y, CP / 4)));
+            vi = (up ? 2 : 0) + (up2 ? 1 : 0);
+          } else if constexpr (PB == 2) {
+            const bool up = (c & (CP / 2)) != 0;
+            kp = up ? ub[1] : ub[0];
+            const C s = up ? ub[0] : ub[1];
+            kp = cadd(kp, mk<C>(__shfl_xor_sync(0xffffffffu, s.x, CP / 2), __shfl_xor_sync(0xffffffffu, s.y, CP / 2)));
+            vi = up ? 1 : 0;
+          }
 #pragma unroll
-        for (int off = CP / 2; off > 0; off >>= 1) {
-          ur += __shfl_xor_sync(0xffffffffu, ur, off);
-          ui += __shfl_xor_sync(0xffffffffu, ui, off);
+          for (int off = CP / (2 * PB); off > 0; off >>= 1) {
+            kp.x += __shfl_xor_sync(0xffffffffu, kp.x, off);
+            kp.y += __shfl_xor_sync(0xffffffffu, kp.y, off);
+          }
+          if ((c & (CP / PB - 1)) == 0) psum[j + (m - (PB - 1) + vi) * T] = kp;
         }
-        if (c == 0) psum[k] = mk<C>(ur, ui);
       }
     }
     v[m] = cscale(cadd(cmul(A, ea2), cmul(Bi, eb2)), h);
